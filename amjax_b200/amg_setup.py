@@ -1,0 +1,345 @@
+"""Host-side AMG hierarchy construction, standing in for PyAMG's solver factories.
+
+The reference never builds a hierarchy itself: ``MultilevelSolver.from_pyamg``
+(amjax/multilevel.py:125-186) converts one made by ``pyamg.smoothed_aggregation_solver``
+or ``pyamg.ruge_stuben_solver`` (benchmarks/benchmark.ipynb cell 5,
+tests/test_multilevel.py:59,82).  PyAMG (``pyamg>=4.0.0``, unpinned in
+pyproject.toml:32) is not importable on these machines, so this module restates the
+published setup algorithms in numpy/scipy and returns an object with PyAMG's shape:
+``.levels[i].A`` (scipy CSR), ``.levels[i].P`` / ``.levels[i].R`` on every level but
+the coarsest.  ``from_pyamg`` accepts either this object or a real PyAMG one.
+
+Algorithms (restated from the literature, not from PyAMG's source):
+
+* Smoothed aggregation (Vanek, Mandel & Brezina, Computing 56, 1996) with PyAMG's
+  documented defaults: symmetric strength with theta = 0, standard (greedy three-pass)
+  aggregation, the constant candidate improved by 4 symmetric Gauss-Seidel sweeps on
+  ``A b = 0`` at the finest level, tentative prolongator from a per-aggregate QR of the
+  candidate, one damped-Jacobi prolongator smoothing step with ``omega = 4/3 / rho(D^-1 A)``,
+  ``R = P^T`` and the Galerkin product ``A_c = R A P``; ``max_levels = 10``,
+  ``max_coarse = 10``.
+* Ruge-Stueben classical AMG (Ruge & Stueben, 1987): classical strength with
+  ``theta = 0.25`` on ``|a_ij|``, the first-pass C/F splitting, direct interpolation,
+  ``R = P^T``, Galerkin coarse operators.
+
+The resulting arrays are NOT bit-identical to PyAMG's (tie-breaking and the spectral
+radius estimate differ); the solve phase only needs some valid hierarchy, and the GPU
+path and the oracle always consume the same arrays.
+"""
+
+from __future__ import annotations
+
+import heapq
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+__all__ = [
+    "HostLevel",
+    "HostHierarchy",
+    "smoothed_aggregation_solver",
+    "ruge_stuben_solver",
+    "save_hierarchy",
+    "load_hierarchy",
+]
+
+
+class HostLevel:
+    """One level of a host hierarchy: ``A`` and, except on the coarsest, ``P`` and ``R``."""
+
+    def __init__(self, A, P=None, R=None):
+        self.A = A
+        if P is not None:
+            self.P = P
+        if R is not None:
+            self.R = R
+
+
+class HostHierarchy:
+    """PyAMG-shaped container: ``levels`` is finest-first, scipy CSR throughout."""
+
+    def __init__(self, levels, kind="unknown"):
+        self.levels = levels
+        self.kind = kind
+
+    def __repr__(self):
+        rows = ", ".join(f"{lvl.A.shape[0]}/{lvl.A.nnz}" for lvl in self.levels)
+        return f"HostHierarchy({self.kind}: rows/nnz per level = {rows})"
+
+
+def _csr(A):
+    A = sp.csr_matrix(A)
+    A.sum_duplicates()
+    A.eliminate_zeros()
+    A.sort_indices()
+    return A
+
+
+def _rho_dinv_a(A):
+    """Largest |eigenvalue| of D^-1 A (ARPACK, with a power-iteration fallback)."""
+    d = A.diagonal()
+    dinv = np.where(d != 0, 1.0 / np.where(d != 0, d, 1.0), 0.0)
+    DA = sp.diags(dinv) @ A
+    n = A.shape[0]
+    if n <= 64:
+        ev = np.linalg.eigvals(DA.toarray())
+        return float(np.max(np.abs(ev)))
+    try:
+        v0 = np.random.default_rng(0).standard_normal(n)
+        ev = spla.eigs(DA, k=1, which="LM", return_eigenvectors=False, v0=v0, tol=1e-4, maxiter=200)
+        return float(np.abs(ev[0]))
+    except Exception:  # ARPACK did not converge: fall back to power iteration
+        v = np.random.default_rng(0).standard_normal(n)
+        v /= np.linalg.norm(v)
+        rho = 1.0
+        for _ in range(50):
+            w = DA @ v
+            rho = np.linalg.norm(w)
+            if rho == 0:
+                break
+            v = w / rho
+        return float(rho)
+
+
+# ---------------------------------------------------------------- smoothed aggregation
+
+def _symmetric_strength(A, theta=0.0):
+    """Keep off-diagonal a_ij with |a_ij| >= theta * sqrt(|a_ii a_jj|) (theta=0 keeps all)."""
+    A = A.tocoo()
+    off = A.row != A.col
+    d = np.abs(_csr(A).diagonal())
+    keep = off & (np.abs(A.data) >= theta * np.sqrt(d[A.row] * d[A.col]))
+    S = sp.csr_matrix((np.ones(keep.sum()), (A.row[keep], A.col[keep])), shape=A.shape)
+    return _csr(S)
+
+
+def _standard_aggregation(S):
+    """Greedy three-pass aggregation on the strength graph S (diagonal-free CSR).
+
+    Pass 1: every node whose neighbours are all free becomes a root; it and its
+    neighbours form an aggregate.  Pass 2: each still-free node joins the aggregate of
+    an aggregated neighbour.  Pass 3: each node still free starts a new aggregate with
+    its free neighbours.  Nodes without neighbours stay unaggregated (index -1).
+    Returns (agg index per node, number of aggregates).
+    """
+    n = S.shape[0]
+    ptr, idx = S.indptr, S.indices
+    agg = np.full(n, -2, dtype=np.int64)  # -2 free, -1 isolated
+    deg = np.diff(ptr)
+    agg[deg == 0] = -1
+    nagg = 0
+    ptr_l = ptr.tolist(); idx_l = idx.tolist(); agg_l = agg.tolist()
+    for i in range(n):
+        if agg_l[i] != -2:
+            continue
+        nb = idx_l[ptr_l[i]:ptr_l[i + 1]]
+        if all(agg_l[j] == -2 for j in nb):
+            agg_l[i] = nagg
+            for j in nb:
+                agg_l[j] = nagg
+            nagg += 1
+    pass2 = agg_l[:]
+    for i in range(n):
+        if agg_l[i] != -2:
+            continue
+        for j in idx_l[ptr_l[i]:ptr_l[i + 1]]:
+            if agg_l[j] >= 0:
+                pass2[i] = agg_l[j]
+                break
+    agg_l = pass2
+    for i in range(n):
+        if agg_l[i] != -2:
+            continue
+        agg_l[i] = nagg
+        for j in idx_l[ptr_l[i]:ptr_l[i + 1]]:
+            if agg_l[j] == -2:
+                agg_l[j] = nagg
+        nagg += 1
+    return np.asarray(agg_l, dtype=np.int64), nagg
+
+
+def _symmetric_gauss_seidel(A, x, b, iterations):
+    """``iterations`` symmetric (forward then backward) point Gauss-Seidel sweeps."""
+    L = sp.tril(A, 0, format="csr")
+    U = sp.triu(A, 0, format="csr")
+    Ls = sp.triu(A, 1, format="csr")
+    Us = sp.tril(A, -1, format="csr")
+    for _ in range(iterations):
+        x = spla.spsolve_triangular(L, b - Ls @ x, lower=True)
+        x = spla.spsolve_triangular(U, b - Us @ x, lower=False)
+    return x
+
+
+def _fit_candidates(agg, nagg, B):
+    """Tentative prolongator T and coarse candidates from a per-aggregate QR of B (1 column)."""
+    n = B.shape[0]
+    member = agg >= 0
+    rows = np.nonzero(member)[0]
+    cols = agg[member]
+    bvals = B[member, 0]
+    norms = np.sqrt(np.bincount(cols, weights=bvals * bvals, minlength=nagg))
+    safe = np.where(norms > 0, norms, 1.0)
+    T = sp.csr_matrix((bvals / safe[cols], (rows, cols)), shape=(n, nagg))
+    return _csr(T), norms.reshape(-1, 1)
+
+
+def smoothed_aggregation_solver(A, B=None, max_levels=10, max_coarse=10, theta=0.0,
+                                improve_iterations=4, omega=4.0 / 3.0, **_ignored):
+    """Build an SA hierarchy with the defaults listed in the module docstring."""
+    A = _csr(A).astype(np.float64)
+    B = np.ones((A.shape[0], 1)) if B is None else np.asarray(B, dtype=np.float64).reshape(A.shape[0], -1)
+    levels = [HostLevel(A)]
+    while len(levels) < max_levels and levels[-1].A.shape[0] > max_coarse:
+        A = levels[-1].A
+        S = _symmetric_strength(A, theta)
+        agg, nagg = _standard_aggregation(S)
+        if nagg == 0 or nagg >= A.shape[0]:
+            break
+        if len(levels) == 1 and improve_iterations:
+            B = _symmetric_gauss_seidel(A, B[:, 0].copy(), np.zeros(A.shape[0]), improve_iterations).reshape(-1, 1)
+        T, Bc = _fit_candidates(agg, nagg, B)
+        d = A.diagonal()
+        dinv = np.where(d != 0, 1.0 / np.where(d != 0, d, 1.0), 0.0)
+        w = omega / _rho_dinv_a(A)
+        P = _csr(T - w * (sp.diags(dinv) @ (A @ T)))
+        R = _csr(P.T)
+        Ac = _csr(R @ A @ P)
+        levels[-1].P = P
+        levels[-1].R = R
+        levels.append(HostLevel(Ac))
+        B = Bc
+    return HostHierarchy(levels, kind="smoothed_aggregation")
+
+
+# ---------------------------------------------------------------- Ruge-Stueben
+
+def _classical_strength(A, theta=0.25):
+    """j strongly influences i when |a_ij| >= theta * max_{k != i} |a_ik| (diagonal dropped)."""
+    A = A.tocoo()
+    off = A.row != A.col
+    r, c, v = A.row[off], A.col[off], np.abs(A.data[off])
+    rmax = np.zeros(A.shape[0])
+    np.maximum.at(rmax, r, v)
+    keep = v >= theta * rmax[r]
+    return _csr(sp.csr_matrix((np.ones(keep.sum()), (r[keep], c[keep])), shape=A.shape))
+
+
+def _rs_first_pass(S):
+    """First-pass Ruge-Stueben C/F splitting.  Returns a bool array, True for C points."""
+    n = S.shape[0]
+    St = _csr(S.T)
+    sp_ptr, sp_idx = S.indptr.tolist(), S.indices.tolist()
+    st_ptr, st_idx = St.indptr.tolist(), St.indices.tolist()
+    lam = np.diff(St.indptr).tolist()
+    state = [0] * n  # 0 unassigned, 1 C, 2 F
+    for i in range(n):
+        if lam[i] == 0 and sp_ptr[i + 1] == sp_ptr[i]:
+            state[i] = 2
+    heap = [(-lam[i], i) for i in range(n) if state[i] == 0]
+    heapq.heapify(heap)
+    while heap:
+        negl, i = heapq.heappop(heap)
+        if state[i] != 0 or -negl != lam[i]:
+            continue
+        state[i] = 1
+        for j in st_idx[st_ptr[i]:st_ptr[i + 1]]:
+            if state[j] == 0:
+                state[j] = 2
+                for k in sp_idx[sp_ptr[j]:sp_ptr[j + 1]]:
+                    if state[k] == 0:
+                        lam[k] += 1
+                        heapq.heappush(heap, (-lam[k], k))
+        for k in sp_idx[sp_ptr[i]:sp_ptr[i + 1]]:
+            if state[k] == 0:
+                lam[k] -= 1
+                heapq.heappush(heap, (-lam[k], k))
+    return np.asarray(state) == 1
+
+
+def _direct_interpolation(A, S, is_c):
+    """Direct interpolation: P_ij = -(alpha_i or beta_i) a_ij / a_ii over strong C neighbours."""
+    n = A.shape[0]
+    cidx = np.cumsum(is_c) - 1
+    nc = int(is_c.sum())
+    Ac = A.tocoo()
+    off = Ac.row != Ac.col
+    r, c, v = Ac.row[off], Ac.col[off], Ac.data[off]
+    diag = A.diagonal()
+    Sset = set(zip(*S.nonzero())) if S.nnz < 2_000_000 else None
+    if Sset is not None:
+        strong = np.fromiter(((ri, ci) in Sset for ri, ci in zip(r.tolist(), c.tolist())), bool, len(r))
+    else:  # large matrices: strength pattern via a sorted-key lookup
+        key = r.astype(np.int64) * n + c
+        Sc = S.tocoo()
+        skey = np.sort(Sc.row.astype(np.int64) * n + Sc.col)
+        pos = np.searchsorted(skey, key)
+        strong = (pos < len(skey)) & (skey[np.minimum(pos, len(skey) - 1)] == key)
+    interp = strong & is_c[c] & ~is_c[r]
+    neg = v < 0
+    sum_neg = np.bincount(r, weights=np.where(neg, v, 0.0), minlength=n)
+    sum_pos = np.bincount(r, weights=np.where(~neg, v, 0.0), minlength=n)
+    csum_neg = np.bincount(r[interp], weights=np.where(neg[interp], v[interp], 0.0), minlength=n)
+    csum_pos = np.bincount(r[interp], weights=np.where(~neg[interp], v[interp], 0.0), minlength=n)
+    alpha = np.where(csum_neg != 0, sum_neg / np.where(csum_neg != 0, csum_neg, 1.0), 0.0)
+    # positive off-diagonals with no positive C partner are lumped into the diagonal
+    beta = np.where(csum_pos != 0, sum_pos / np.where(csum_pos != 0, csum_pos, 1.0), 0.0)
+    dmod = diag + np.where(csum_pos == 0, sum_pos, 0.0)
+    ri, ci, vi = r[interp], c[interp], v[interp]
+    w = -np.where(vi < 0, alpha[ri], beta[ri]) * vi / dmod[ri]
+    crow = np.nonzero(is_c)[0]
+    rows = np.concatenate([crow, ri])
+    cols = np.concatenate([cidx[crow], cidx[ci]])
+    vals = np.concatenate([np.ones(nc), w])
+    return _csr(sp.csr_matrix((vals, (rows, cols)), shape=(n, nc)))
+
+
+def ruge_stuben_solver(A, max_levels=10, max_coarse=10, theta=0.25, **_ignored):
+    """Build a classical (Ruge-Stueben) hierarchy with the defaults in the module docstring."""
+    A = _csr(A).astype(np.float64)
+    levels = [HostLevel(A)]
+    while len(levels) < max_levels and levels[-1].A.shape[0] > max_coarse:
+        A = levels[-1].A
+        S = _classical_strength(A, theta)
+        is_c = _rs_first_pass(S)
+        nc = int(is_c.sum())
+        if nc == 0 or nc >= A.shape[0]:
+            break
+        P = _direct_interpolation(A, S, is_c)
+        R = _csr(P.T)
+        levels[-1].P = P
+        levels[-1].R = R
+        levels.append(HostLevel(_csr(R @ A @ P)))
+    return HostHierarchy(levels, kind="ruge_stuben")
+
+
+# ---------------------------------------------------------------- serialisation
+
+def save_hierarchy(path, hierarchy):
+    """Write every level's CSR arrays to one ``.npz`` (replayable on any machine)."""
+    out = {"n_levels": np.array(len(hierarchy.levels)), "kind": np.array(getattr(hierarchy, "kind", ""))}
+    for i, lvl in enumerate(hierarchy.levels):
+        for name in ("A", "P", "R"):
+            M = getattr(lvl, name, None)
+            if M is None:
+                continue
+            M = _csr(M)
+            out[f"{name}{i}_data"] = M.data
+            out[f"{name}{i}_indices"] = M.indices.astype(np.int32)
+            out[f"{name}{i}_indptr"] = M.indptr.astype(np.int64)
+            out[f"{name}{i}_shape"] = np.array(M.shape)
+    np.savez_compressed(path, **out)
+
+
+def load_hierarchy(path):
+    """Inverse of :func:`save_hierarchy`."""
+    z = np.load(path, allow_pickle=False)
+    levels = []
+    for i in range(int(z["n_levels"])):
+        mats = {}
+        for name in ("A", "P", "R"):
+            if f"{name}{i}_data" in z:
+                mats[name] = sp.csr_matrix((z[f"{name}{i}_data"], z[f"{name}{i}_indices"], z[f"{name}{i}_indptr"]),
+                                           shape=tuple(z[f"{name}{i}_shape"]))
+        levels.append(HostLevel(mats["A"], mats.get("P"), mats.get("R")))
+    return HostHierarchy(levels, kind=str(z["kind"]))

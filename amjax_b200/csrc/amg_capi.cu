@@ -1,0 +1,250 @@
+// amg_capi.cu -- the C ABI (include/amg_b200.h) over the runtime.
+#include "amg_runtime.cuh"
+
+// ======================================================================= C ABI
+using namespace amg;
+
+template <class T>
+static void jacobi_impl(const amg_csr* Ad, const void* x, const void* b, const void* dinv, void* out,
+                        int k, int iterations, double omega, cudaStream_t s) {
+  Csr A(*Ad);
+  T* tmp = nullptr;
+  const size_t bytes = size_t(A.n_rows) * k * sizeof(T);
+  if (iterations > 1) CK(cudaMallocAsync(reinterpret_cast<void**>(&tmp), bytes, s));
+  try {
+    const T* in = static_cast<const T*>(x);
+    for (int i = 0; i < iterations; ++i) {
+      T* o = ((iterations - 1 - i) % 2 == 0) ? static_cast<T*>(out) : tmp;
+      OpJacobi<T, XS_PLAIN> op{};
+      op.xs = XSource<T, XS_PLAIN>{in, static_cast<const T*>(b), static_cast<const T*>(dinv), T(omega), k};
+      op.b = static_cast<const T*>(b);
+      op.dinv = static_cast<const T*>(dinv);
+      op.omega = T(omega);
+      op.out = o;
+      op.ld = k;
+      run_csr(A, op, k, Red{}, s, {in, b, o});
+      in = o;
+    }
+  } catch (...) {
+    if (tmp) cudaFreeAsync(tmp, s);
+    throw;
+  }
+  if (tmp) CK(cudaFreeAsync(tmp, s));
+}
+
+
+extern "C" {
+
+amg_status amg_hierarchy_create(const amg_level_desc* levels, int32_t n_levels,
+                                const amg_coarse_desc* coarse, amg_hierarchy** out) {
+  return guarded([&] {
+    if (!out || !levels || !coarse) fail(AMG_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (n_levels < 2) fail(AMG_ERR_UNSUPPORTED, "a hierarchy needs at least 2 levels (got %d)", n_levels);
+    auto h = std::make_unique<amg_hierarchy>();
+    for (int l = 0; l < n_levels; ++l) {
+      const amg_level_desc& d = levels[l];
+      check_csr(d.A, "A", l);
+      if (d.A.n_rows != d.A.n_cols) fail(AMG_ERR_INVALID_ARG, "level %d: A is not square", l);
+      Level lv;
+      lv.A = Csr(d.A);
+      if (l < n_levels - 1) {
+        check_csr(d.P, "P", l);
+        check_csr(d.R, "R", l);
+        const int nc = levels[l + 1].A.n_rows;
+        if (d.P.n_rows != d.A.n_rows || d.P.n_cols != nc)
+          fail(AMG_ERR_INVALID_ARG, "level %d: P is %dx%d, expected %dx%d", l, d.P.n_rows, d.P.n_cols, d.A.n_rows, nc);
+        if (d.R.n_rows != nc || d.R.n_cols != d.A.n_rows)
+          fail(AMG_ERR_INVALID_ARG, "level %d: R is %dx%d, expected %dx%d", l, d.R.n_rows, d.R.n_cols, nc, d.A.n_rows);
+        lv.P = Csr(d.P);
+        lv.R = Csr(d.R);
+        for (const amg_smoother* sm : {&d.pre, &d.post})
+          if (sm->kind != AMG_SMOOTH_NONE && sm->kind != AMG_SMOOTH_JACOBI)
+            fail(AMG_ERR_INVALID_ARG, "level %d: unknown smoother kind %d", l, sm->kind);
+        lv.pre = Smooth{d.pre.kind, d.pre.iterations, d.pre.omega};
+        lv.post = Smooth{d.post.kind, d.post.iterations, d.post.omega};
+      }
+      lv.dinv64 = d.dinv64;
+      lv.dinv32 = d.dinv32;
+      h->levels.push_back(lv);
+    }
+    Coarse c;
+    c.kind = coarse->kind;
+    c.n = coarse->n;
+    c.m0_64 = coarse->m0_64; c.m0_32 = coarse->m0_32;
+    c.m1_64 = coarse->m1_64; c.m1_32 = coarse->m1_32;
+    c.perm = coarse->perm;
+    c.iters = coarse->iterations;
+    c.omega = coarse->omega;
+    if (c.kind < AMG_COARSE_PINV || c.kind > AMG_COARSE_JACOBI)
+      fail(AMG_ERR_INVALID_ARG, "unknown coarse solver kind %d", c.kind);
+    if (c.n != h->levels.back().A.n_rows)
+      fail(AMG_ERR_INVALID_ARG, "coarse n=%d does not match the coarsest level (%d)", c.n, h->levels.back().A.n_rows);
+    if (c.kind == AMG_COARSE_LU && !c.perm) fail(AMG_ERR_INVALID_ARG, "LU coarse solver needs perm");
+    h->coarse = c;
+    *out = h.release();
+  });
+}
+
+amg_status amg_hierarchy_destroy(amg_hierarchy* h) {
+  return guarded([&] { delete h; });
+}
+
+amg_status amg_solve(amg_hierarchy* h, int32_t precision, const void* b, void* x, int32_t k,
+                     double tol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
+                     const amg_csr* A0, int32_t* iters_out, double* relres_out, void* stream) {
+  return guarded([&] {
+    if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
+    check_vec(b, "b");
+    check_vec(x, "x");
+    if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
+    if (maxiter < 0) fail(AMG_ERR_INVALID_ARG, "maxiter must be >= 0");
+    cycle_char(cycle);
+    std::lock_guard<std::mutex> lk(h->mu);
+    Csr a0;
+    const Csr* pa0 = nullptr;
+    if (A0) { a0 = override_csr(h, A0); pa0 = &a0; }
+    check_prec_data(h, precision, pa0);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Plan* pl = get_plan(h, precision, k, s);
+    Req q{precision, k, cycle, cycles_per_level, maxiter, tol, 0.0, b, x, pa0};
+    if (precision == AMG_PREC_F64) solve_plain<double>(h, pl, q, s);
+    else if (precision == AMG_PREC_F32) solve_plain<float>(h, pl, q, s);
+    else if (precision == AMG_PREC_MIXED) solve_mixed(h, pl, q, s);
+    else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
+    read_results(pl, s, false, iters_out, relres_out);
+  });
+}
+
+amg_status amg_precondition(amg_hierarchy* h, int32_t precision, const void* b, void* x,
+                            int32_t k, int32_t cycle, int32_t cycles_per_level, void* stream) {
+  return guarded([&] {
+    if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
+    check_vec(b, "b");
+    check_vec(x, "x");
+    if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
+    cycle_char(cycle);
+    std::lock_guard<std::mutex> lk(h->mu);
+    const int cprec = precision == AMG_PREC_F64 ? AMG_PREC_F64 : AMG_PREC_F32;
+    check_prec_data(h, cprec, nullptr);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Plan* pl = get_plan(h, precision, k, s);
+    Req q{precision, k, cycle, cycles_per_level, 0, 0.0, 0.0, b, x, nullptr};
+    if (precision == AMG_PREC_F64) precondition<double>(h, pl, q, s);
+    else if (precision == AMG_PREC_F32 || precision == AMG_PREC_MIXED) precondition<float>(h, pl, q, s);
+    else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
+  });
+}
+
+amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, int32_t k,
+                   double tol, double atol, int32_t maxiter, int32_t cycle,
+                   int32_t cycles_per_level, const amg_csr* A0, int32_t* iters_out,
+                   double* relres_out, void* stream) {
+  return guarded([&] {
+    if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
+    check_vec(b, "b");
+    check_vec(x, "x");
+    if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
+    if (maxiter < 0) fail(AMG_ERR_INVALID_ARG, "maxiter must be >= 0");
+    cycle_char(cycle);
+    std::lock_guard<std::mutex> lk(h->mu);
+    Csr a0;
+    const Csr* pa0 = nullptr;
+    if (A0) { a0 = override_csr(h, A0); pa0 = &a0; }
+    check_prec_data(h, precision, nullptr);
+    if (pa0 && (precision == AMG_PREC_F32 ? !pa0->v32 : !pa0->v64))
+      fail(AMG_ERR_INVALID_ARG, "A0 lacks values for this precision");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Plan* pl = get_plan(h, precision, k, s);
+    Req q{precision, k, cycle, cycles_per_level, maxiter, tol, atol, b, x, pa0};
+    if (precision == AMG_PREC_F64) pcg<double, double>(h, pl, q, s);
+    else if (precision == AMG_PREC_F32) pcg<float, float>(h, pl, q, s);
+    else if (precision == AMG_PREC_MIXED) pcg<double, float>(h, pl, q, s);
+    else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
+    read_results(pl, s, true, iters_out, relres_out);
+  });
+}
+
+amg_status amg_jacobi(const amg_csr* A, int32_t dtype, const void* x, const void* b,
+                      const void* dinv, void* out, int32_t k, int32_t iterations, double omega,
+                      void* stream) {
+  return guarded([&] {
+    if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
+    check_csr(*A, "A", 0);
+    check_vec(x, "x"); check_vec(b, "b"); check_vec(dinv, "dinv"); check_vec(out, "out");
+    if (x == out) fail(AMG_ERR_INVALID_ARG, "out may not alias x");
+    if (k < 1 || iterations < 0) fail(AMG_ERR_INVALID_ARG, "bad k or iterations");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (iterations == 0) {
+      const size_t es = dtype == 0 ? 8 : 4;
+      CK(cudaMemcpyAsync(out, x, size_t(A->n_rows) * k * es, cudaMemcpyDeviceToDevice, s));
+      return;
+    }
+    if (dtype == 0) jacobi_impl<double>(A, x, b, dinv, out, k, iterations, omega, s);
+    else if (dtype == 1) jacobi_impl<float>(A, x, b, dinv, out, k, iterations, omega, s);
+    else fail(AMG_ERR_INVALID_ARG, "dtype must be 0 (FP64) or 1 (FP32)");
+  });
+}
+
+amg_status amg_spmv(const amg_csr* A, int32_t dtype, const void* x, void* y, int32_t k, void* stream) {
+  return guarded([&] {
+    if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
+    check_csr(*A, "A", 0);
+    check_vec(x, "x"); check_vec(y, "y");
+    if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Csr M(*A);
+    if (dtype == 0) {
+      OpAxpy<double, XS_ZERO> op{};
+      op.x = static_cast<const double*>(x); op.out = static_cast<double*>(y); op.ld = k;
+      run_csr(M, op, k, Red{}, s, {x, y});
+    } else if (dtype == 1) {
+      OpAxpy<float, XS_ZERO> op{};
+      op.x = static_cast<const float*>(x); op.out = static_cast<float*>(y); op.ld = k;
+      run_csr(M, op, k, Red{}, s, {x, y});
+    } else {
+      fail(AMG_ERR_INVALID_ARG, "dtype must be 0 (FP64) or 1 (FP32)");
+    }
+  });
+}
+
+amg_status amg_inverse_diagonal(const amg_csr* A, int32_t dtype, void* dinv, void* stream) {
+  return guarded([&] {
+    if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
+    check_csr(*A, "A", 0);
+    check_vec(dinv, "dinv");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int grid = std::max(1, std::min((A->n_rows + 255) / 256, dev_info().max_ctas));
+    if (dtype == 0) inv_diag_kernel<double><<<grid, 256, 0, s>>>(A->rowptr, A->col, A->val64, A->n_rows, static_cast<double*>(dinv));
+    else if (dtype == 1) inv_diag_kernel<float><<<grid, 256, 0, s>>>(A->rowptr, A->col, A->val32, A->n_rows, static_cast<float*>(dinv));
+    else fail(AMG_ERR_INVALID_ARG, "dtype must be 0 (FP64) or 1 (FP32)");
+    CK_LAUNCH();
+  });
+}
+
+amg_status amg_sampled_outer(const amg_csr* A, const double* lam, const double* x, int32_t k,
+                             double* grad, void* stream) {
+  return guarded([&] {
+    if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
+    check_csr(*A, "A", 0);
+    check_vec(lam, "lam"); check_vec(x, "x"); check_vec(grad, "grad");
+    if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int grid = std::max(1, std::min((A->n_rows + 7) / 8, dev_info().max_ctas));
+    sampled_outer_kernel<<<grid, 256, 0, s>>>(A->rowptr, A->col, A->n_rows, lam, x, k, grad);
+    CK_LAUNCH();
+  });
+}
+
+int64_t amg_kernel_launch_count(void) {
+  if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+  unsigned long long mine = 0;
+  if (cudaMemcpyFromSymbol(&mine, g_kernel_count, sizeof(mine)) != cudaSuccess) return -1;
+  return int64_t(mine + count_f64() + count_f32() + count_mixed() + count_runtime());
+}
+
+const char* amg_last_error(void) { return t_err.c_str(); }
+
+const char* amg_version(void) { return "amg_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,92 @@
+// amg_drv_f32.cu -- FP32 solve drivers (the reference's dtype=float32 mode; also the FP32 preconditioner).
+#include "amg_runtime.cuh"
+
+namespace amg {
+
+// Standalone solve, one precision end to end (F64 or F32).
+template <class T>
+void solve_plain(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
+  const int n0 = h->levels[0].A.n_rows;
+  const T* b = static_cast<const T*>(q.b);
+  T* x = static_cast<T*>(q.x);
+  const char ct = cycle_char(q.cycle);
+  const Csr* A0 = q.A0 ? q.A0 : &h->levels[0].A;
+  auto prologue = [&](cudaStream_t cs) {
+    emit_setup<T, T, 0>(pl, cs, n0, b, nullptr, nullptr, x, q.tol, 0.0, q.maxiter);
+  };
+  auto body = [&](cudaStream_t cs) {
+    Cycle<T> cy{};
+    cy.h = h; cy.pl = pl; cy.s = cs; cy.k = q.k; cy.stop = pl->stop(); cy.A0 = A0;
+    cy.b0 = b; cy.x0 = x; cy.fine_norm = true; cy.ctl = make_ctl(pl, q.maxiter);
+    cy.fine_mask = q.k > 1; cy.red = red_of(pl);
+    cy.visit(0, false, ct, q.cpl);
+  };
+  run_loop(pl, req_key("solve", q), user, prologue, body, [](cudaStream_t) {}, true, q.maxiter + 2);
+}
+
+// Preconditioned CG (outer type TO, cycle type TC).
+template <class TO, class TC>
+void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
+  const int n0 = h->levels[0].A.n_rows;
+  const TO* b = static_cast<const TO*>(q.b);
+  TO* x = static_cast<TO*>(q.x);
+  TO* r = static_cast<TO*>(pl->r_out);
+  TO* p = static_cast<TO*>(pl->p_out);
+  TO* qv = static_cast<TO*>(pl->q_out);
+  constexpr bool mixed = !std::is_same<TO, TC>::value;
+  TC* rc = mixed ? static_cast<TC*>(pl->B[0]) : reinterpret_cast<TC*>(r);
+  TC* z = static_cast<TC*>(pl->X[0]);
+  const char ct = cycle_char(q.cycle);
+  const Csr* A0 = q.A0 ? q.A0 : &h->levels[0].A;
+  auto cycle = [&](cudaStream_t cs) {
+    Cycle<TC> cy{};
+    cy.h = h; cy.pl = pl; cy.s = cs; cy.k = q.k; cy.stop = pl->stop(); cy.A0 = nullptr;
+    cy.b0 = rc; cy.x0 = z; cy.fine_dot = r; cy.dot_is_f64 = sizeof(TO) == 8;
+    cy.red = red_of(pl);
+    cy.visit(0, true, ct, q.cpl);
+  };
+  auto prologue = [&](cudaStream_t cs) {
+    emit_setup<TO, TC, 1>(pl, cs, n0, b, r, mixed ? rc : nullptr, x, q.tol, q.atol, q.maxiter);
+    cycle(cs);
+    OpConvert<TO, TC> cp{z, p, q.k, pl->stop()};
+    run_elem<TC>(n0, cp, q.k, red_of(pl), cs, {z, p});
+  };
+  auto body = [&](cudaStream_t cs) {
+    OpCgQ<TO> qop{p, qv, q.k, pl->stop(), pl->gamma(), pl->alpha()};
+    run_csr(*A0, qop, q.k, red_of(pl), cs, {p, qv});
+    OpCgUpdate<TO, TC> up{};
+    up.x = x; up.r = r; up.p = p; up.q = qv; up.r_lo = mixed ? rc : nullptr;
+    up.alpha = pl->alpha(); up.active = pl->active(); up.ld = q.k; up.stop = pl->stop();
+    up.ctl = make_ctl(pl, q.maxiter);
+    run_elem<TC>(n0, up, q.k, red_of(pl), cs, {x, r, p, qv, up.r_lo});
+    cycle(cs);
+    OpCgDir<TO, TC> dir{p, z, pl->beta(), q.k, pl->stop()};
+    run_elem<TC>(n0, dir, q.k, red_of(pl), cs, {p, z});
+  };
+  run_loop(pl, req_key("pcg", q), user, prologue, body, [](cudaStream_t) {}, true, q.maxiter + 2);
+}
+
+template <class T>
+void precondition(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
+  const char ct = cycle_char(q.cycle);
+  auto prologue = [&](cudaStream_t cs) {
+    Cycle<T> cy{};
+    cy.h = h; cy.pl = pl; cy.s = cs; cy.k = q.k; cy.stop = nullptr; cy.A0 = nullptr;
+    cy.b0 = static_cast<const T*>(q.b); cy.x0 = static_cast<T*>(q.x); cy.red = red_of(pl);
+    cy.visit(0, true, ct, q.cpl);
+  };
+  run_loop(pl, req_key("prec", q), user, prologue, [](cudaStream_t) {}, [](cudaStream_t) {}, false, 0);
+}
+
+
+template void solve_plain<float>(amg_hierarchy*, Plan*, const Req&, cudaStream_t);
+template void pcg<float, float>(amg_hierarchy*, Plan*, const Req&, cudaStream_t);
+template void precondition<float>(amg_hierarchy*, Plan*, const Req&, cudaStream_t);
+
+unsigned long long count_f32() {
+  unsigned long long v = 0;
+  cudaMemcpyFromSymbol(&v, g_kernel_count, sizeof(v));
+  return v;
+}
+
+}  // namespace amg

@@ -1,0 +1,352 @@
+// amg_runtime.cu -- non-template host runtime: errors, device facts, plans, graph
+// construction (conditional WHILE node) and execution.
+#include "amg_runtime.cuh"
+
+namespace amg {
+
+thread_local std::string t_err;
+
+[[noreturn]] void fail(amg_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw Error{st, std::string(buf)};
+}
+
+DevInfo dev_info() {
+  static std::mutex m;
+  static std::map<int, DevInfo> cache;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(m);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  DevInfo d;
+  CK(cudaDeviceGetAttribute(&d.nsm, cudaDevAttrMultiProcessorCount, dev));
+  d.max_ctas = d.nsm * (2048 / kBlock);
+  cache[dev] = d;
+  return d;
+}
+
+void check_csr(const amg_csr& c, const char* what, int lvl) {
+  if (c.n_rows < 0 || c.n_cols < 0 || c.nnz < 0)
+    fail(AMG_ERR_INVALID_ARG, "level %d %s: negative size", lvl, what);
+  if (c.nnz > INT32_MAX) fail(AMG_ERR_UNSUPPORTED, "level %d %s: nnz exceeds int32", lvl, what);
+  if (c.n_rows > 0 && (!c.rowptr || (c.nnz > 0 && !c.col)))
+    fail(AMG_ERR_INVALID_ARG, "level %d %s: null rowptr/col", lvl, what);
+  if (c.nnz > 0 && !c.val64 && !c.val32)
+    fail(AMG_ERR_INVALID_ARG, "level %d %s: no values", lvl, what);
+}
+
+// Loop guard: ends each body of the device while-loop.  Sets the loop condition from
+// the stop flag and a hard trip bound, so the loop always terminates.
+__global__ void loop_guard_kernel(int* stop, int* gcount, int gmax, cudaGraphConditionalHandle h) {
+  count_launch();
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const int g = ++(*gcount);
+    const int cont = (*stop == 0) && (g < gmax);
+    if (!cont) *stop = 1;
+    cudaGraphSetConditional(h, cont ? 1u : 0u);
+  }
+}
+
+// Host-loop variant of the guard (no conditional node).
+__global__ void loop_guard_host_kernel(int* stop, int* gcount, int gmax) {
+  count_launch();
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const int g = ++(*gcount);
+    if (!((*stop == 0) && (g < gmax))) *stop = 1;
+  }
+}
+
+// ------------------------------------------------------------------ plans
+static std::string plan_key(int prec, int k, cudaStream_t s) {
+  char buf[96];
+  snprintf(buf, sizeof(buf), "%d/%d/%p", prec, k, (void*)s);
+  return buf;
+}
+
+Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s) {
+  const std::string key = plan_key(prec, k, s);
+  auto it = h->plans.find(key);
+  if (it != h->plans.end()) return it->second.get();
+  auto pl = std::make_unique<Plan>();
+  pl->prec = prec;
+  pl->k = k;
+  pl->stream = s;
+  CK(cudaGetDevice(&pl->dev));
+  pl->csize = (prec == AMG_PREC_F64) ? 8 : 4;
+  const size_t osize = (prec == AMG_PREC_F32) ? 4 : 8;
+  const int L = int(h->levels.size());
+  for (int l = 0; l < L; ++l) {
+    const size_t n = size_t(h->levels[l].A.n_rows) * k;
+    pl->X.push_back(pl->alloc(n * pl->csize));
+    pl->B.push_back(pl->alloc(n * pl->csize));
+    pl->W1.push_back(pl->alloc(n * pl->csize));
+    pl->W2.push_back(pl->alloc(n * pl->csize));
+  }
+  const size_t n0 = size_t(h->levels[0].A.n_rows) * k;
+  pl->r_out = pl->alloc(n0 * osize);
+  pl->p_out = pl->alloc(n0 * osize);
+  pl->q_out = pl->alloc(n0 * osize);
+  pl->dscal = static_cast<double*>(pl->alloc(sizeof(double) * 6 * k));
+  pl->iscal = static_cast<int*>(pl->alloc(sizeof(int) * (2 * k + 2)));
+  CK(cudaMemset(pl->iscal, 0, sizeof(int) * (2 * k + 2)));
+  pl->partials = static_cast<double*>(pl->alloc(sizeof(double) * size_t(dev_info().max_ctas) * k));
+  pl->counter = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * 4));
+  CK(cudaMemset(pl->counter, 0, sizeof(unsigned) * 4));
+  CK(cudaHostAlloc(reinterpret_cast<void**>(&pl->h_stop), sizeof(int), cudaHostAllocDefault));
+  Plan* raw = pl.get();
+  h->plans[key] = std::move(pl);
+  return raw;
+}
+
+// ------------------------------------------------------------------ execution
+enum ExecMode { EXEC_GRAPH = 0, EXEC_HOSTLOOP = 1, EXEC_EAGER = 2 };
+
+static ExecMode exec_mode() {
+  const char* e = std::getenv("AMG_EXEC");
+  if (!e) return EXEC_GRAPH;
+  if (!strcmp(e, "hostloop")) return EXEC_HOSTLOOP;
+  if (!strcmp(e, "eager")) return EXEC_EAGER;
+  return EXEC_GRAPH;
+}
+
+// A private stream for stream capture (the caller's stream may be the legacy default
+// stream, which cannot be captured).
+static cudaStream_t capture_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  streams[dev] = s;
+  return s;
+}
+
+template <class F>
+static cudaGraph_t capture(cudaGraph_t into, const cudaGraphNode_t* deps, size_t ndeps, F&& f) {
+  cudaStream_t cs = capture_stream();
+  CK(cudaStreamBeginCaptureToGraph(cs, into, deps, nullptr, ndeps, cudaStreamCaptureModeThreadLocal));
+  try {
+    f(cs);
+  } catch (...) {
+    cudaGraph_t junk = into;
+    cudaStreamEndCapture(cs, &junk);
+    throw;
+  }
+  cudaGraph_t out = into;
+  CK(cudaStreamEndCapture(cs, &out));
+  return out;
+}
+
+static std::vector<cudaGraphNode_t> sinks(cudaGraph_t g) {
+  size_t n = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n), out;
+  if (n) CK(cudaGraphGetNodes(g, nodes.data(), &n));
+  for (auto nd : nodes) {
+    size_t d = 0;
+    CK(cudaGraphNodeGetDependentNodes(nd, nullptr, &d));
+    if (d == 0) out.push_back(nd);
+  }
+  return out;
+}
+
+static int64_t count_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &n));
+  return int64_t(n);
+}
+
+
+// Build (or fetch) and run prologue; while(any column active) body; epilogue.
+void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& prologue,
+                     const Emit& body, const Emit& epilogue, bool has_loop, int gmax) {
+  const ExecMode mode = exec_mode();
+  if (mode == EXEC_EAGER) {
+    prologue(user);
+    if (has_loop) {
+      for (int trip = 0;; ++trip) {
+        body(user);
+        loop_guard_host_kernel<<<1, 32, 0, user>>>(pl->stop(), pl->gcount(), gmax);
+        CK_LAUNCH();
+        CK(cudaMemcpyAsync(pl->h_stop, pl->stop(), sizeof(int), cudaMemcpyDeviceToHost, user));
+        CK(cudaStreamSynchronize(user));
+        if (*pl->h_stop) break;
+      }
+    }
+    epilogue(user);
+    CK_LAUNCH();
+    return;
+  }
+  // graph cache lookup (LRU of 8)
+  GraphEntry* ge = nullptr;
+  for (auto it = pl->graphs.begin(); it != pl->graphs.end(); ++it) {
+    if (it->first == key) {
+      pl->graphs.splice(pl->graphs.begin(), pl->graphs, it);
+      ge = pl->graphs.front().second.get();
+      break;
+    }
+  }
+  if (!ge) {
+    auto e = std::make_unique<GraphEntry>();
+    if (mode == EXEC_GRAPH || !has_loop) {
+      cudaGraph_t g;
+      CK(cudaGraphCreate(&g, 0));
+      e->graph = g;
+      capture(g, nullptr, 0, prologue);
+      if (has_loop) {
+        std::vector<cudaGraphNode_t> dep = sinks(g);
+        cudaGraphConditionalHandle hc;
+        CK(cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = hc;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cn;
+        CK(cudaGraphAddNode(&cn, g, dep.empty() ? nullptr : dep.data(), dep.size(), &cp));
+        cudaGraph_t bg = cp.conditional.phGraph_out[0];
+        int* stp = pl->stop();
+        int* gc = pl->gcount();
+        capture(bg, nullptr, 0, [&](cudaStream_t cs) {
+          body(cs);
+          loop_guard_kernel<<<1, 32, 0, cs>>>(stp, gc, gmax, hc);
+          CK_LAUNCH();
+        });
+        pl->nodes_body = count_nodes(bg);
+        capture(g, &cn, 1, epilogue);
+      } else {
+        pl->nodes_body = 0;
+      }
+      CK(cudaGraphInstantiate(&e->exec, g, 0));
+    } else {  // host loop: prologue+epilogue graph pieces, body graph
+      e->host_loop = true;
+      cudaGraph_t g;
+      CK(cudaGraphCreate(&g, 0));
+      e->graph = g;
+      capture(g, nullptr, 0, prologue);
+      CK(cudaGraphInstantiate(&e->exec, g, 0));
+      cudaGraph_t bg;
+      CK(cudaGraphCreate(&bg, 0));
+      e->body = bg;
+      int* stp = pl->stop();
+      int* gc = pl->gcount();
+      capture(bg, nullptr, 0, [&](cudaStream_t cs) {
+        body(cs);
+        loop_guard_host_kernel<<<1, 32, 0, cs>>>(stp, gc, gmax);
+        CK_LAUNCH();
+      });
+      CK(cudaGraphInstantiate(&e->body_exec, bg, 0));
+    }
+    pl->graphs.emplace_front(key, std::move(e));
+    while (pl->graphs.size() > 8) pl->graphs.pop_back();
+    ge = pl->graphs.front().second.get();
+  }
+  if (!ge->host_loop) {
+    CK(cudaGraphLaunch(ge->exec, user));
+  } else {
+    CK(cudaGraphLaunch(ge->exec, user));
+    for (;;) {
+      CK(cudaGraphLaunch(ge->body_exec, user));
+      CK(cudaMemcpyAsync(pl->h_stop, pl->stop(), sizeof(int), cudaMemcpyDeviceToHost, user));
+      CK(cudaStreamSynchronize(user));
+      if (*pl->h_stop) break;
+    }
+    epilogue(user);  // epilogues are empty or direct launches
+    CK_LAUNCH();
+  }
+}
+
+void read_results(Plan* pl, cudaStream_t s, bool cg, int32_t* iters_out, double* relres_out) {
+  if (!iters_out && !relres_out) return;
+  const int k = pl->k;
+  std::vector<int> it(k);
+  std::vector<double> nr(k), nb(k);
+  CK(cudaMemcpyAsync(it.data(), pl->iters(), sizeof(int) * k, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nr.data(), pl->nr(), sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nb.data(), pl->normb(), sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int c = 0; c < k; ++c) {
+    if (iters_out) iters_out[c] = it[c];
+    if (relres_out) relres_out[c] = (cg ? std::sqrt(nr[c]) : nr[c]) / nb[c];
+  }
+}
+
+LoopCtl make_ctl(Plan* pl, int maxiter) {
+  LoopCtl c{};
+  c.nr = pl->nr();
+  c.thresh = pl->thresh();
+  c.active = pl->active();
+  c.iters = pl->iters();
+  c.stop = pl->stop();
+  c.maxiter = maxiter;
+  return c;
+}
+
+Red red_of(Plan* pl) { return Red{pl->partials, pl->counter}; }
+
+char cycle_char(int cycle) {
+  if (cycle == AMG_CYCLE_V) return 'V';
+  if (cycle == AMG_CYCLE_W) return 'W';
+  if (cycle == AMG_CYCLE_F) return 'F';
+  fail(AMG_ERR_INVALID_ARG, "Cycle %d not supported. Use 'V', 'W', or 'F'.", cycle);
+}
+
+std::string req_key(const char* kind, const Req& q) {
+  char buf[320];
+  snprintf(buf, sizeof(buf), "%s/%d/%d/%d/%d/%d/%.17g/%.17g/%p/%p/%p/%p/%p/%p", kind, q.prec, q.k,
+           q.cycle, q.cpl, q.maxiter, q.tol, q.atol, q.b, (void*)q.x,
+           q.A0 ? (const void*)q.A0->rowptr : nullptr, q.A0 ? (const void*)q.A0->col : nullptr,
+           q.A0 ? (const void*)q.A0->v64 : nullptr, q.A0 ? (const void*)q.A0->v32 : nullptr);
+  return buf;
+}
+
+void check_prec_data(amg_hierarchy* h, int prec, const Csr* A0) {
+  const int L = int(h->levels.size());
+  for (int l = 0; l < L; ++l) {
+    const Level& lv = h->levels[l];
+    const bool need64 = prec == AMG_PREC_F64;
+    auto has = [&](const Csr& M) { return M.nnz == 0 || (need64 ? M.v64 != nullptr : M.v32 != nullptr); };
+    const Csr& A = (l == 0 && A0) ? *A0 : lv.A;
+    if (!has(A) || (l < L - 1 && (!has(lv.P) || !has(lv.R))))
+      fail(AMG_ERR_INVALID_ARG, "level %d lacks %s matrix values", l, need64 ? "FP64" : "FP32");
+    if (need64 ? !lv.dinv64 : !lv.dinv32) fail(AMG_ERR_INVALID_ARG, "level %d lacks dinv", l);
+  }
+  if (prec == AMG_PREC_MIXED) {
+    const Csr& A = A0 ? *A0 : h->levels[0].A;
+    if (!A.v64) fail(AMG_ERR_INVALID_ARG, "MIXED needs FP64 values of the level-0 operator");
+  }
+  const Coarse& c = h->coarse;
+  const bool need64 = prec == AMG_PREC_F64;
+  if (c.kind != AMG_COARSE_JACOBI && (need64 ? !c.m0_64 : !c.m0_32))
+    fail(AMG_ERR_INVALID_ARG, "coarse solver data missing for this precision");
+  if (c.kind == AMG_COARSE_QR && (need64 ? !c.m1_64 : !c.m1_32))
+    fail(AMG_ERR_INVALID_ARG, "coarse QR factor R missing for this precision");
+}
+
+Csr override_csr(amg_hierarchy* h, const amg_csr* A0) {
+  check_csr(*A0, "A0", 0);
+  const Csr& A = h->levels[0].A;
+  if (A0->n_rows != A.n_rows || A0->n_cols != A.n_cols)
+    fail(AMG_ERR_INVALID_ARG, "A0 shape %dx%d does not match level 0 (%dx%d)", A0->n_rows, A0->n_cols,
+         A.n_rows, A.n_cols);
+  return Csr(*A0);
+}
+
+void check_vec(const void* p, const char* name) {
+  if (!p) fail(AMG_ERR_INVALID_ARG, "%s is null", name);
+}
+
+
+unsigned long long count_runtime() {
+  unsigned long long v = 0;
+  cudaMemcpyFromSymbol(&v, g_kernel_count, sizeof(v));
+  return v;
+}
+
+}  // namespace amg

@@ -1,0 +1,664 @@
+// amg_runtime.cuh -- host runtime of the B200 multigrid solve phase (shared by the
+// per-precision translation units and the C ABI).
+//
+// A hierarchy handle wraps caller-owned device CSR arrays.  A "plan" (per precision,
+// number of right-hand sides k and stream) owns the per-level work vectors, the
+// per-column loop state and the reduction scratch.  Each solve is emitted once as a
+// CUDA graph: the cycle's level recursion (V, W, F) is unrolled at capture time into a
+// static sequence of fused CSR kernels, and the outer loop is a conditional WHILE node
+// whose condition the kernels set on the device, so a whole solve is one graph launch
+// with no host round trip.  Graphs are cached per (solve kind, parameters, buffers).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <type_traits>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/amg_b200.h"
+#include "amg_device.cuh"
+
+namespace amg {
+
+// ------------------------------------------------------------------ errors
+extern thread_local std::string t_err;
+
+struct Error {
+  amg_status st;
+  std::string msg;
+};
+
+[[noreturn]] void fail(amg_status st, const char* fmt, ...);
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      fail(AMG_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+           __LINE__);                                                                   \
+  } while (0)
+
+#define CK_LAUNCH() CK(cudaGetLastError())
+
+template <class F>
+static amg_status guarded(F&& f) {
+  try {
+    f();
+    t_err.clear();
+    return AMG_OK;
+  } catch (const Error& e) {
+    t_err = e.msg;
+    return e.st;
+  } catch (const std::exception& e) {
+    t_err = e.what();
+    return AMG_ERR_CUDA;
+  }
+}
+
+// ------------------------------------------------------------------ device facts
+struct DevInfo {
+  int nsm = 148;
+  int max_ctas = 148 * 8;
+};
+
+DevInfo dev_info();
+
+// ------------------------------------------------------------------ CSR view
+struct Csr {
+  int n_rows = 0, n_cols = 0;
+  int64_t nnz = 0;
+  const int* rowptr = nullptr;
+  const int* col = nullptr;
+  const double* v64 = nullptr;
+  const float* v32 = nullptr;
+  int g1 = 4;  // threads per row for k == 1
+
+  Csr() = default;
+  explicit Csr(const amg_csr& c) {
+    n_rows = c.n_rows;
+    n_cols = c.n_cols;
+    nnz = c.nnz;
+    rowptr = c.rowptr;
+    col = c.col;
+    v64 = c.val64;
+    v32 = c.val32;
+    const double mean = n_rows > 0 ? double(nnz) / n_rows : 0.0;
+    g1 = mean < 1.5 ? 1 : mean < 3 ? 2 : mean < 6 ? 4 : mean < 12 ? 8 : mean < 24 ? 16 : 32;
+  }
+  template <class T>
+  const T* vals() const {
+    if constexpr (sizeof(T) == 8) return reinterpret_cast<const T*>(v64);
+    else return reinterpret_cast<const T*>(v32);
+  }
+};
+
+void check_csr(const amg_csr& c, const char* what, int lvl);
+
+// ------------------------------------------------------------------ hierarchy
+struct Smooth {
+  int kind = AMG_SMOOTH_NONE;
+  int iters = 0;
+  double omega = 1.0;
+  bool on() const { return kind == AMG_SMOOTH_JACOBI && iters > 0; }
+};
+
+struct Level {
+  Csr A, P, R;
+  const double* dinv64 = nullptr;
+  const float* dinv32 = nullptr;
+  Smooth pre, post;
+  template <class T>
+  const T* dinv() const {
+    if constexpr (sizeof(T) == 8) return reinterpret_cast<const T*>(dinv64);
+    else return reinterpret_cast<const T*>(dinv32);
+  }
+};
+
+struct Coarse {
+  int kind = AMG_COARSE_PINV;
+  int n = 0;
+  const double* m0_64 = nullptr;
+  const float* m0_32 = nullptr;
+  const double* m1_64 = nullptr;
+  const float* m1_32 = nullptr;
+  const int* perm = nullptr;
+  int iters = 10;
+  double omega = 1.0;
+  template <class T>
+  const T* m0() const {
+    if constexpr (sizeof(T) == 8) return reinterpret_cast<const T*>(m0_64);
+    else return reinterpret_cast<const T*>(m0_32);
+  }
+  template <class T>
+  const T* m1() const {
+    if constexpr (sizeof(T) == 8) return reinterpret_cast<const T*>(m1_64);
+    else return reinterpret_cast<const T*>(m1_32);
+  }
+};
+
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t body = nullptr;        // host-loop mode
+  cudaGraphExec_t body_exec = nullptr;
+  bool host_loop = false;
+  ~GraphEntry() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (body_exec) cudaGraphExecDestroy(body_exec);
+    if (body) cudaGraphDestroy(body);
+  }
+};
+
+struct Plan {
+  int prec = 0, k = 1;
+  cudaStream_t stream = nullptr;
+  int dev = 0;
+  size_t csize = 8;                   // bytes of the cycle's type
+  std::vector<void*> X, B, W1, W2;    // per level, cycle type
+  void* r_out = nullptr;              // outer residual (outer type)
+  void* p_out = nullptr;
+  void* q_out = nullptr;
+  void* r_lo = nullptr;               // cycle-type copy of r (MIXED)
+  double* dscal = nullptr;            // per-column doubles: thresh, nr, normb, gamma, alpha, beta
+  int* iscal = nullptr;               // per-column ints: active, iters; then stop, gcount
+  double* partials = nullptr;
+  unsigned* counter = nullptr;
+  int* h_stop = nullptr;              // pinned host mirror of the stop flag (host-loop mode)
+  std::vector<void*> allocs;
+  std::list<std::pair<std::string, std::unique_ptr<GraphEntry>>> graphs;  // LRU
+  int64_t nodes_outside = 0, nodes_body = 0;
+
+  double* thresh() { return dscal; }
+  double* nr() { return dscal + k; }
+  double* normb() { return dscal + 2 * k; }
+  double* gamma() { return dscal + 3 * k; }
+  double* alpha() { return dscal + 4 * k; }
+  double* beta() { return dscal + 5 * k; }
+  int* active() { return iscal; }
+  int* iters() { return iscal + k; }
+  int* stop() { return iscal + 2 * k; }
+  int* gcount() { return iscal + 2 * k + 1; }
+
+  void* alloc(size_t bytes) {
+    void* p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(bytes, 256)));
+    allocs.push_back(p);
+    return p;
+  }
+  ~Plan() {
+    graphs.clear();
+    for (void* p : allocs) cudaFree(p);
+    if (h_stop) cudaFreeHost(h_stop);
+  }
+};
+
+}  // namespace amg
+
+struct amg_hierarchy {
+  std::vector<amg::Level> levels;
+  amg::Coarse coarse;
+  std::mutex mu;
+  std::map<std::string, std::unique_ptr<amg::Plan>> plans;
+};
+
+namespace amg {
+
+// ------------------------------------------------------------------ launch helpers
+struct Cfg {
+  int G = 1, KV = 1, grid = 1;
+  size_t smem = 0;
+};
+
+static int pow2ceil(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+template <class T>
+static int pick_kv(int k, std::initializer_list<const void*> ptrs) {
+  if (k == 1) return 1;
+  int kv = (sizeof(T) == 8) ? 2 : 4;
+  while (kv > 1 && (k % kv) != 0) kv >>= 1;
+  for (const void* p : ptrs)
+    while (kv > 1 && (reinterpret_cast<uintptr_t>(p) % (sizeof(T) * kv)) != 0) kv >>= 1;
+  return kv;
+}
+
+template <class T>
+static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> ptrs) {
+  Cfg c;
+  const DevInfo d = dev_info();
+  if (k == 1) {
+    c.G = g1;
+    c.KV = 1;
+  } else {
+    c.KV = pick_kv<T>(k, ptrs);
+    const int nch = k / c.KV;
+    c.G = std::max(4, std::min(32, pow2ceil(nch)));
+    if ((nch + c.G - 1) / c.G > kMaxCh)
+      fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);
+    c.smem = sizeof(double) * std::max<size_t>(size_t(kBlock / c.G) * k, kBlock);
+  }
+  const int rows_per_cta = kBlock / c.G;
+  const int64_t need = (int64_t(n_rows) + rows_per_cta - 1) / rows_per_cta;
+  c.grid = int(std::max<int64_t>(1, std::min<int64_t>(need, d.max_ctas)));
+  return c;
+}
+
+struct Red {
+  double* partials = nullptr;
+  unsigned* counter = nullptr;
+};
+
+template <class Op, int G>
+static void launch_k1(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
+                      RedCtx rc, cudaStream_t s) {
+  csr_k1<Op, G><<<c.grid, kBlock, 0, s>>>(M.rowptr, M.col, vals, M.n_rows, op, rc);
+}
+
+template <class Op, int G, int KV>
+static void launch_kb(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
+                      RedCtx rc, cudaStream_t s) {
+  csr_kb<Op, G, KV><<<c.grid, kBlock, c.smem, s>>>(M.rowptr, M.col, vals, M.n_rows, op, rc);
+}
+
+template <class Op, int KV>
+static void dispatch_kb_g(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
+                          RedCtx rc, cudaStream_t s) {
+  switch (c.G) {
+    case 4: launch_kb<Op, 4, KV>(M, vals, op, c, rc, s); break;
+    case 8: launch_kb<Op, 8, KV>(M, vals, op, c, rc, s); break;
+    case 16: launch_kb<Op, 16, KV>(M, vals, op, c, rc, s); break;
+    default: launch_kb<Op, 32, KV>(M, vals, op, c, rc, s); break;
+  }
+}
+
+// Launch one fused CSR pass of matrix M with epilogue op over k columns.
+template <class Op>
+static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
+                    std::initializer_list<const void*> ptrs) {
+  using V = typename Op::V;
+  const V* vals = M.template vals<V>();
+  if (M.nnz > 0 && !vals) fail(AMG_ERR_INVALID_ARG, "matrix values missing for this precision");
+  const Cfg c = cfg_k<typename Op::Acc>(M.n_rows, k, M.g1, ptrs);
+  RedCtx rc{red.partials, red.counter, k};
+  if (op.reduces() && !red.partials) fail(AMG_ERR_INVALID_ARG, "reduction scratch missing");
+  if (k == 1) {
+    switch (c.G) {
+      case 1: launch_k1<Op, 1>(M, vals, op, c, rc, s); break;
+      case 2: launch_k1<Op, 2>(M, vals, op, c, rc, s); break;
+      case 4: launch_k1<Op, 4>(M, vals, op, c, rc, s); break;
+      case 8: launch_k1<Op, 8>(M, vals, op, c, rc, s); break;
+      case 16: launch_k1<Op, 16>(M, vals, op, c, rc, s); break;
+      default: launch_k1<Op, 32>(M, vals, op, c, rc, s); break;
+    }
+  } else {
+    switch (c.KV) {
+      case 1: dispatch_kb_g<Op, 1>(M, vals, op, c, rc, s); break;
+      case 2: dispatch_kb_g<Op, 2>(M, vals, op, c, rc, s); break;
+      default: dispatch_kb_g<Op, 4>(M, vals, op, c, rc, s); break;
+    }
+  }
+  CK_LAUNCH();
+}
+
+template <class Op, int G, int KV>
+static void launch_elem(int n, const Op& op, const Cfg& c, RedCtx rc, cudaStream_t s) {
+  elem_kb<Op, G, KV><<<c.grid, kBlock, c.smem, s>>>(n, op, rc);
+}
+
+template <class Op, int KV>
+static void dispatch_elem_g(int n, const Op& op, const Cfg& c, RedCtx rc, cudaStream_t s) {
+  switch (c.G) {
+    case 1: launch_elem<Op, 1, KV>(n, op, c, rc, s); break;
+    case 4: launch_elem<Op, 4, KV>(n, op, c, rc, s); break;
+    case 8: launch_elem<Op, 8, KV>(n, op, c, rc, s); break;
+    case 16: launch_elem<Op, 16, KV>(n, op, c, rc, s); break;
+    default: launch_elem<Op, 32, KV>(n, op, c, rc, s); break;
+  }
+}
+
+// Elementwise pass over [n, k]; T_align is the narrowest element type the op touches
+// (it bounds the vector width).
+template <class TA, class Op>
+static void run_elem(int n, const Op& op, int k, const Red& red, cudaStream_t s,
+                     std::initializer_list<const void*> ptrs) {
+  Cfg c = cfg_k<TA>(n, k, 1, ptrs);
+  if (k == 1) c.G = 1;
+  if (k == 1) {
+    const int64_t need = (int64_t(n) + kBlock - 1) / kBlock;
+    c.grid = int(std::max<int64_t>(1, std::min<int64_t>(need, dev_info().max_ctas)));
+  }
+  RedCtx rc{red.partials, red.counter, k};
+  if (op.reduces() && !red.partials) fail(AMG_ERR_INVALID_ARG, "reduction scratch missing");
+  switch (c.KV) {
+    case 1: dispatch_elem_g<Op, 1>(n, op, c, rc, s); break;
+    case 2: dispatch_elem_g<Op, 2>(n, op, c, rc, s); break;
+    default: dispatch_elem_g<Op, 4>(n, op, c, rc, s); break;
+  }
+  CK_LAUNCH();
+}
+
+// ------------------------------------------------------------------ cycle emission
+// How the SpMV sees an iterate: a stored vector, one Jacobi sweep from zero computed
+// on the fly, or the zero vector.
+template <class T>
+struct XD {
+  int kind = XS_ZERO;
+  const T* p = nullptr;
+  static XD plain(const T* q) { XD d; d.kind = XS_PLAIN; d.p = q; return d; }
+  static XD jac0() { XD d; d.kind = XS_JAC0; return d; }
+  static XD zero() { XD d; d.kind = XS_ZERO; return d; }
+};
+
+template <class T>
+struct Cycle {
+  amg_hierarchy* h;
+  Plan* pl;
+  cudaStream_t s;
+  int k;
+  const int* stop;         // checked by every cycle kernel (nullable)
+  const Csr* A0;           // level-0 operator (override or the hierarchy's)
+  const T* b0;             // level-0 right-hand side
+  T* x0;                   // level-0 iterate / result
+  bool fine_norm = false;  // standalone: fuse ||b - A x|| into the first level-0 sweep
+  LoopCtl ctl{};
+  bool fine_mask = false;  // write level-0 result only for active columns
+  const void* fine_dot = nullptr;  // CG: fuse <r, z> into the last level-0 sweep (outer type)
+  bool dot_is_f64 = true;
+  Red red;
+
+  int L() const { return int(h->levels.size()); }
+  const Csr& Aof(int l) const { return (l == 0 && A0) ? *A0 : h->levels[l].A; }
+  T* Xb(int l) const { return l == 0 ? x0 : static_cast<T*>(pl->X[l]); }
+  const T* Bb(int l) const { return l == 0 ? b0 : static_cast<const T*>(pl->B[l]); }
+  T* W1(int l) const { return static_cast<T*>(pl->W1[l]); }
+  T* W2(int l) const { return static_cast<T*>(pl->W2[l]); }
+
+  template <int XS>
+  XSource<T, XS> xsrc(int l, const T* xp, T omega) const {
+    const Level& lv = h->levels[l];
+    return XSource<T, XS>{xp, Bb(l), lv.template dinv<T>(), omega, k};
+  }
+
+  // One Jacobi sweep in -> out on level l; flags select the fused extras.
+  template <int XS>
+  void sweep_x(int l, const T* in, T omega, T* out, bool norm, bool mask, bool dot) {
+    const Level& lv = h->levels[l];
+    OpJacobi<T, XS> op{};
+    op.xs = xsrc<XS>(l, in, omega);
+    op.b = Bb(l);
+    op.dinv = lv.template dinv<T>();
+    op.omega = omega;
+    op.out = out;
+    op.ld = k;
+    op.norm = norm ? 1 : 0;
+    op.active = mask ? pl->active() : nullptr;
+    op.stop = norm ? nullptr : stop;
+    op.rdot64 = (dot && dot_is_f64) ? static_cast<const double*>(fine_dot) : nullptr;
+    op.rdot32 = (dot && !dot_is_f64) ? static_cast<const float*>(fine_dot) : nullptr;
+    op.ctl = ctl;
+    op.gamma = pl->gamma();
+    op.beta = pl->beta();
+    run_csr(Aof(l), op, k, red, s, {in, Bb(l), out, dot ? fine_dot : nullptr});
+  }
+
+  void sweep(int l, XD<T> in, T omega, T* out, bool norm, bool mask, bool dot) {
+    if (in.kind == XS_PLAIN) sweep_x<XS_PLAIN>(l, in.p, omega, out, norm, mask, dot);
+    else if (in.kind == XS_JAC0) sweep_x<XS_JAC0>(l, nullptr, omega, out, norm, mask, dot);
+    else fail(AMG_ERR_INVALID_ARG, "internal: sweep from the zero vector");
+  }
+
+  // n sweeps starting from `src`; the last writes `dst`, the others alternate between
+  // t_a and t_b so that no sweep reads the buffer it writes.  `src` is never written.
+  void sweeps(int l, XD<T> src, int n, T omega, T* dst, T* t_a, T* t_b, bool norm_first,
+              bool mask_last, bool dot_last) {
+    if (n <= 0) return;
+    // choose the order of temps so the last intermediate is not dst
+    T* ta = t_a;
+    T* tb = t_b;
+    if (n >= 2) {
+      T* last_inter = ((n - 2) % 2 == 0) ? ta : tb;
+      if (last_inter == dst) std::swap(ta, tb);
+    }
+    XD<T> in = src;
+    for (int i = 0; i < n; ++i) {
+      const bool last = (i == n - 1);
+      T* out = last ? dst : ((i % 2 == 0) ? ta : tb);
+      if (in.kind == XS_PLAIN && in.p == out) fail(AMG_ERR_INVALID_ARG, "internal: sweep aliasing");
+      sweep(l, in, omega, out, norm_first && i == 0, mask_last && last, dot_last && last);
+      in = XD<T>::plain(out);
+    }
+  }
+
+  template <int XS, bool NORM>
+  void resid_t(int l, const T* xp, T omega, const T* b, T* out) {
+    OpResid<T, T, XS, true, T, NORM> op{};
+    op.xs = xsrc<XS>(l, xp, omega);
+    op.b = b;
+    op.out = out;
+    op.out_lo = nullptr;
+    op.ld = k;
+    op.stop = NORM ? nullptr : stop;
+    op.ctl = ctl;
+    run_csr(Aof(l), op, k, red, s, {xp, b, out});
+  }
+
+  template <int BS>
+  void axpy_t(const Csr& M, const T* base, T omega, int l_base, const T* x, T* out) {
+    OpAxpy<T, BS> op{};
+    op.base = xsrc<BS>(l_base, base, omega);
+    op.x = x;
+    op.out = out;
+    op.ld = k;
+    op.stop = stop;
+    run_csr(M, op, k, red, s, {base, x, out});
+  }
+
+  // Level 0 without a post-smoother but with a mask or a fused CG dot: finish with an
+  // elementwise pass dst = src (active columns) that also reduces <r, z>.
+  template <class TR, bool DOT>
+  void elem_copy_t(int n, const T* src, T* dst, bool mask) {
+    OpMaskCopy<T, TR, DOT> op{};
+    op.src = src;
+    op.dst = dst;
+    op.active = mask ? pl->active() : nullptr;
+    op.ld = k;
+    op.stop = stop;
+    op.rdot = static_cast<const TR*>(fine_dot);
+    op.gamma = pl->gamma();
+    op.beta = pl->beta();
+    run_elem<T>(n, op, k, red, s, {src, dst, fine_dot});
+  }
+  void elem_copy(int n, const T* src, T* dst, bool mask, bool dot) {
+    if (!dot) elem_copy_t<double, false>(n, src, dst, mask);
+    else if (dot_is_f64) elem_copy_t<double, true>(n, src, dst, mask);
+    else elem_copy_t<float, true>(n, src, dst, mask);
+  }
+
+  void norm_only(int l, const T* xp) {
+    OpResid<T, T, XS_PLAIN, false, T, true> op{};
+    op.xs = xsrc<XS_PLAIN>(l, xp, T(1));
+    op.b = Bb(l);
+    op.out = nullptr;
+    op.out_lo = nullptr;
+    op.ld = k;
+    op.stop = nullptr;
+    op.ctl = ctl;
+    run_csr(Aof(l), op, k, red, s, {xp, Bb(l)});
+  }
+
+  void coarse_solve(const T* b, T* x) {
+    const Coarse& c = h->coarse;
+    const int l = L() - 1;
+    const int n = h->levels[l].A.n_rows;
+    const int tot = n * k;
+    const int grid = std::max(1, std::min((tot + 127) / 128, dev_info().max_ctas));
+    if (c.kind == AMG_COARSE_PINV) {
+      coarse_gemv<T><<<grid, 128, 0, s>>>(c.template m0<T>(), b, x, n, k, 0, stop);
+    } else if (c.kind == AMG_COARSE_LU) {
+      coarse_trsv<T, 0><<<(k + 63) / 64, 64, 0, s>>>(c.template m0<T>(), c.perm, b, x, n, k, stop);
+    } else if (c.kind == AMG_COARSE_QR) {
+      coarse_gemv<T><<<grid, 128, 0, s>>>(c.template m0<T>(), b, x, n, k, 1, stop);
+      CK_LAUNCH();
+      coarse_trsv<T, 1><<<(k + 63) / 64, 64, 0, s>>>(c.template m1<T>(), nullptr, x, x, n, k, stop);
+    } else {  // Jacobi sweeps from zero on the coarsest operator
+      const T om = T(c.omega);
+      // level l's own right-hand side buffer is b (== B[l]); sweeps read Bb(l)
+      if (c.iters <= 0) {
+        OpJac0<T> z{b, h->levels[l].template dinv<T>(), T(0), x, k, stop};
+        run_elem<T>(n, z, k, red, s, {b, x});
+      } else if (c.iters == 1) {
+        OpJac0<T> z{b, h->levels[l].template dinv<T>(), om, x, k, stop};
+        run_elem<T>(n, z, k, red, s, {b, x});
+      } else {
+        sweeps(l, XD<T>::jac0(), c.iters - 1, om, x, W1(l), W2(l), false, false, false);
+      }
+    }
+    CK_LAUNCH();
+  }
+
+  // One visit of level l (multilevel.py:316-337).  x_zero: the incoming iterate is 0.
+  // On return the new iterate is in Xb(l).
+  void visit(int l, bool x_zero, char ct, int cpl) {
+    const Level& lv = h->levels[l];
+    const int n = lv.A.n_rows;
+    T* X = Xb(l);
+    const T* B = Bb(l);
+    T* w1 = W1(l);
+    T* w2 = W2(l);
+    const bool top = (l == 0);
+
+    // ---- pre-smoothing (x1)
+    XD<T> x1 = x_zero ? XD<T>::zero() : XD<T>::plain(X);
+    const bool fuse_norm = top && fine_norm && !x_zero && lv.pre.on();
+    if (top && fine_norm && !fuse_norm) norm_only(0, x_zero ? nullptr : X);
+    if (lv.pre.on()) {
+      const T om = T(lv.pre.omega);
+      if (x_zero) {
+        if (lv.pre.iters == 1) x1 = XD<T>::jac0();
+        else {
+          sweeps(l, XD<T>::jac0(), lv.pre.iters - 1, om, w1, w2, w1, false, false, false);
+          x1 = XD<T>::plain(w1);
+        }
+      } else {
+        sweeps(l, XD<T>::plain(X), lv.pre.iters, om, w1, w2, w1, fuse_norm, false, false);
+        x1 = XD<T>::plain(w1);
+      }
+    }
+    const T om_pre = T(lv.pre.omega);
+
+    // ---- residual and restriction: b_c = R (b - A x1)
+    const T* r = B;
+    if (x1.kind != XS_ZERO) {
+      if (x1.kind == XS_PLAIN) resid_t<XS_PLAIN, false>(l, x1.p, om_pre, B, w2);
+      else resid_t<XS_JAC0, false>(l, nullptr, om_pre, B, w2);
+      r = w2;
+    }
+    T* Bc = static_cast<T*>(pl->B[l + 1]);
+    axpy_t<XS_ZERO>(lv.R, nullptr, T(0), l, r, Bc);
+
+    // ---- coarse correction
+    T* Xc = static_cast<T*>(pl->X[l + 1]);
+    if (l == L() - 2) {
+      coarse_solve(Bc, Xc);
+    } else if (ct == 'V') {
+      visit(l + 1, true, 'V', cpl);
+    } else if (ct == 'W') {
+      visit(l + 1, true, 'W', cpl);
+      visit(l + 1, false, 'W', cpl);
+    } else {
+      visit(l + 1, true, 'F', cpl);
+      for (int i = 0; i < cpl; ++i) visit(l + 1, false, 'V', cpl);
+    }
+
+    // ---- prolongation + correction: x2 = x1 + P x_c
+    const bool post_on = lv.post.on();
+    const bool need_fix = top && (fine_mask || fine_dot) && !post_on;
+    T* dst2 = (post_on || need_fix) ? w1 : X;
+    if (x1.kind == XS_PLAIN) axpy_t<XS_PLAIN>(lv.P, x1.p, T(0), l, Xc, dst2);
+    else if (x1.kind == XS_JAC0) axpy_t<XS_JAC0>(lv.P, nullptr, om_pre, l, Xc, dst2);
+    else axpy_t<XS_ZERO>(lv.P, nullptr, T(0), l, Xc, dst2);
+
+    // ---- post-smoothing into X
+    if (post_on) {
+      sweeps(l, XD<T>::plain(w1), lv.post.iters, T(lv.post.omega), X, w2, w1, false,
+             top && fine_mask, top && fine_dot != nullptr);
+    } else if (need_fix) {
+      elem_copy(n, w1, X, fine_mask, fine_dot != nullptr);
+    }
+  }
+};
+
+
+// ------------------------------------------------------------------ runtime (amg_runtime.cu)
+using Emit = std::function<void(cudaStream_t)>;
+Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s);
+void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& prologue,
+              const Emit& body, const Emit& epilogue, bool has_loop, int gmax);
+void read_results(Plan* pl, cudaStream_t s, bool cg, int32_t* iters_out, double* relres_out);
+LoopCtl make_ctl(Plan* pl, int maxiter);
+Red red_of(Plan* pl);
+char cycle_char(int cycle);
+void check_prec_data(amg_hierarchy* h, int prec, const Csr* A0);
+Csr override_csr(amg_hierarchy* h, const amg_csr* A0);
+void check_vec(const void* p, const char* name);
+
+struct Req {
+  int prec, k, cycle, cpl, maxiter;
+  double tol, atol;
+  const void* b;
+  void* x;
+  const Csr* A0;
+};
+
+std::string req_key(const char* kind, const Req& q);
+
+template <class T, class TLO, int MODE>
+inline void emit_setup(Plan* pl, cudaStream_t cs, int n0, const T* b, T* dst, TLO* dst_lo, T* zero,
+                       double tol, double atol, int maxiter) {
+  OpSetup<T, TLO, MODE> op{};
+  op.src = b;
+  op.dst = dst;
+  op.dst_lo = dst_lo;
+  op.zero = zero;
+  op.ld = pl->k;
+  op.thresh = pl->thresh();
+  op.nr = pl->nr();
+  op.normb = pl->normb();
+  op.active = pl->active();
+  op.iters = pl->iters();
+  op.stop = pl->stop();
+  op.gcount = pl->gcount();
+  op.tol = tol;
+  op.atol = atol;
+  op.maxiter = maxiter;
+  run_elem<TLO>(n0, op, pl->k, red_of(pl), cs, {b, dst, dst_lo, zero});
+}
+
+// ------------------------------------------------------------------ drivers
+template <class T> void solve_plain(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
+void solve_mixed(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
+template <class TO, class TC> void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
+template <class T> void precondition(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
+
+// per-translation-unit kernel counters (each TU owns a copy of g_kernel_count)
+unsigned long long count_f64();
+unsigned long long count_f32();
+unsigned long long count_mixed();
+unsigned long long count_runtime();
+unsigned long long count_capi();
+
+}  // namespace amg

@@ -1,0 +1,170 @@
+/*
+ * amg_b200.h -- C ABI of the B200 (sm_100a) multigrid solve phase.
+ *
+ * The reference (AMJax) exposes its solve phase as Python methods on
+ * ``MultilevelSolver``; this ABI is what a binding of those methods calls.  Each entry
+ * point names the reference interface it replaces (paths relative to the AMJax root).
+ *
+ * Conventions
+ *  - Every pointer in a descriptor or argument is a DEVICE pointer unless stated.
+ *  - The library never frees caller buffers.  Hierarchy arrays must stay alive and
+ *    unchanged for the life of the hierarchy handle.
+ *  - Vectors with k right-hand sides are stored row-major [n, k] (k contiguous).
+ *  - All work is issued on the caller's stream (``stream`` is a cudaStream_t; NULL means
+ *    the legacy default stream).
+ *  - Functions return an ``amg_status``; no C++ exception crosses the ABI.
+ *    ``amg_last_error()`` gives a human-readable message for the calling thread.
+ *  - Non-convergence is not an error (the reference returns x silently,
+ *    amjax/multilevel.py:414-425); per-column iteration counts and final relative
+ *    residuals are reported through ``iters_out`` / ``relres_out`` (host arrays of
+ *    length k, may be NULL).
+ */
+#ifndef AMG_B200_H
+#define AMG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  AMG_OK = 0,
+  AMG_ERR_INVALID_ARG = 1,   /* bad size, null pointer, unknown enum value */
+  AMG_ERR_UNSUPPORTED = 2,   /* valid request this build does not implement */
+  AMG_ERR_CUDA = 3,          /* a CUDA runtime call failed (message has the detail) */
+  AMG_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+  AMG_ERR_BAD_MATRIX = 5     /* CSR validation failed (unsorted/out-of-range/short) */
+} amg_status;
+
+typedef enum { AMG_CYCLE_V = 0, AMG_CYCLE_W = 1, AMG_CYCLE_F = 2 } amg_cycle;
+
+/* Precision of a solve.
+ *  F64:   every vector, value and accumulation in FP64.
+ *  F32:   FP32 hierarchy end to end (the reference's dtype=float32 mode); sums that
+ *         decide convergence are accumulated in FP64.
+ *  MIXED: the cycle runs on FP32 values and vectors with FP32 accumulation; the outer
+ *         loop (residual b - A x, refinement update, PCG dots/step lengths and the
+ *         convergence norm) runs in FP64 on FP64 values. */
+typedef enum { AMG_PREC_F64 = 0, AMG_PREC_F32 = 1, AMG_PREC_MIXED = 2 } amg_precision;
+
+typedef enum { AMG_SMOOTH_NONE = 0, AMG_SMOOTH_JACOBI = 1 } amg_smoother_kind;
+
+typedef enum {
+  AMG_COARSE_PINV = 0,    /* x = A_inv b         (multilevel.py:509-516) */
+  AMG_COARSE_LU = 1,      /* x = lu_solve(b)     (multilevel.py:519-526) */
+  AMG_COARSE_QR = 2,      /* x = R^-1 Q^T b      (multilevel.py:529-536) */
+  AMG_COARSE_JACOBI = 3   /* Jacobi sweeps from 0 (multilevel.py:501-507) */
+} amg_coarse_kind;
+
+/* One CSR matrix.  rowptr has n_rows+1 entries (int32), col nnz entries (int32,
+ * sorted within a row is not required).  val64 / val32 hold the same values in FP64 /
+ * FP32; a precision mode needs the one(s) it reads (F64: val64; F32: val32; MIXED: both
+ * on level 0's A, val32 elsewhere). */
+typedef struct {
+  int32_t n_rows, n_cols;
+  int64_t nnz;
+  const int32_t* rowptr;
+  const int32_t* col;
+  const double* val64;
+  const float* val32;
+} amg_csr;
+
+typedef struct {
+  int32_t kind;       /* amg_smoother_kind */
+  int32_t iterations; /* sweeps */
+  double omega;       /* damping, already divided by rho when withrho was asked */
+} amg_smoother;
+
+/* One level.  P and R are ignored on the coarsest level. */
+typedef struct {
+  amg_csr A, P, R;
+  const double* dinv64;
+  const float* dinv32;
+  amg_smoother pre, post;
+} amg_level_desc;
+
+/* Coarsest-level solver.  Dense matrices are row-major n x n in both precisions.
+ *  PINV: m0 = A_inv.   LU: m0 = packed LU factors (unit-lower L below the diagonal),
+ *  perm = row permutation (int32, perm[i] = row of b to place at i).
+ *  QR: m0 = Q, m1 = R (upper).   JACOBI: uses the coarsest A/dinv, iterations, omega. */
+typedef struct {
+  int32_t kind;
+  int32_t n;
+  const double* m0_64; const float* m0_32;
+  const double* m1_64; const float* m1_32;
+  const int32_t* perm;
+  int32_t iterations;
+  double omega;
+} amg_coarse_desc;
+
+typedef struct amg_hierarchy amg_hierarchy;
+
+/* Create a hierarchy handle over caller-owned device arrays (the arrays uploaded once
+ * by MultilevelSolver.from_pyamg, amjax/multilevel.py:125-186 / _convert_hierarchy
+ * :557-590).  Validates sizes; the arrays are not copied. */
+amg_status amg_hierarchy_create(const amg_level_desc* levels, int32_t n_levels,
+                                const amg_coarse_desc* coarse, amg_hierarchy** out);
+amg_status amg_hierarchy_destroy(amg_hierarchy* h);
+
+/* Standalone solve: repeated cycles until ||b - A x|| < tol ||b|| per column or
+ * maxiter cycles (MultilevelSolver.solve / _solve_loop, amjax/multilevel.py:341-425).
+ * b, x: [n0, k] in FP64 for F64 and MIXED, FP32 for F32.  x is output only (x0 = 0;
+ * the caller shifts b for a nonzero x0 as multilevel.py:384-394 does).
+ * A0 (nullable) replaces the level-0 operator for smoothing and residuals
+ * (the ``A=`` argument, multilevel.py:318,387-391); it must have A's shape.
+ * Columns freeze independently once converged, as jax.vmap over the while-loop does. */
+amg_status amg_solve(amg_hierarchy* h, int32_t precision, const void* b, void* x, int32_t k,
+                     double tol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
+                     const amg_csr* A0, int32_t* iters_out, double* relres_out, void* stream);
+
+/* One cycle from the zero vector: x = M b (MultilevelSolver.aspreconditioner,
+ * amjax/multilevel.py:265-288).  b, x in the cycle's type: FP64 for F64, FP32 for F32
+ * and MIXED. */
+amg_status amg_precondition(amg_hierarchy* h, int32_t precision, const void* b, void* x,
+                            int32_t k, int32_t cycle, int32_t cycles_per_level, void* stream);
+
+/* Preconditioned CG with M = one cycle (jax.scipy.sparse.linalg.cg(A, b, M=ml.
+ * aspreconditioner()) as the reference's benchmark calls it, benchmarks/benchmark.ipynb
+ * cell 7; stopping rule <r,r> <= max(tol^2 <b,b>, atol^2)).  b, x FP64 ([n0,k]) for F64
+ * and MIXED (FP32 preconditioner inside an FP64 CG), FP32 for F32.  A0 as in amg_solve
+ * (used for the CG operator; the preconditioner keeps the hierarchy's level 0). */
+amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, int32_t k,
+                   double tol, double atol, int32_t maxiter, int32_t cycle,
+                   int32_t cycles_per_level, const amg_csr* A0, int32_t* iters_out,
+                   double* relres_out, void* stream);
+
+/* Damped Jacobi sweeps on one CSR matrix (amjax/relaxation/relaxation.py:64-98).
+ * dtype 0 = FP64 (x, b, dinv, out double), 1 = FP32.  out may not alias x. */
+amg_status amg_jacobi(const amg_csr* A, int32_t dtype, const void* x, const void* b,
+                      const void* dinv, void* out, int32_t k, int32_t iterations,
+                      double omega, void* stream);
+
+/* y = A x for [n_cols, k] x (the BCOO ``A @ x`` of the reference, multilevel.py:321,335). */
+amg_status amg_spmv(const amg_csr* A, int32_t dtype, const void* x, void* y, int32_t k,
+                    void* stream);
+
+/* dinv = 1/diag(A), 0 where the diagonal is 0 (relaxation.py:36-61).  Duplicated
+ * diagonal entries are summed. */
+amg_status amg_inverse_diagonal(const amg_csr* A, int32_t dtype, void* dinv, void* stream);
+
+/* Gradient of a loss through x = A^-1 b with respect to A's stored values: the
+ * reference returns the dense -outer(lambda, x) (multilevel.py:438-442); this samples it
+ * on the pattern: grad[e] = -sum_c lam[row(e), c] * x[col(e), c].  FP64. */
+amg_status amg_sampled_outer(const amg_csr* A, const double* lam, const double* x, int32_t k,
+                             double* grad, void* stream);
+
+/* Number of kernels this library launched in the calling process (monotone counter;
+ * one CUDA-graph launch counts every kernel node it contains). */
+int64_t amg_kernel_launch_count(void);
+
+/* Last error message of the calling thread ("" when none). */
+const char* amg_last_error(void);
+
+/* Library version string. */
+const char* amg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMG_B200_H */
