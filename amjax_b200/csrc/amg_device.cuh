@@ -24,7 +24,14 @@ constexpr int kMaxCh = 4;       // column chunks per lane (k <= 32 * kMaxCh * KV
 // the benchmark reports is read from here, so it counts what actually ran.
 static __device__ unsigned long long g_kernel_count = 0;
 
+// Kernel entry: wait for the preceding grid (programmatic dependent launch: this grid may
+// have been launched while its predecessor was still finishing; griddepcontrol.wait
+// returns once the predecessor has completed and its memory is visible, and at once when
+// there is no programmatic predecessor), then let the next grid start launching, and
+// count the launch.
 __device__ __forceinline__ void count_launch() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&g_kernel_count, 1ull);
 }
 
@@ -75,47 +82,100 @@ __device__ __forceinline__ void ld_cvt(const S* __restrict__ p, T (&v)[KV]) {
 }
 
 // ------------------------------------------------------------------ reductions
+// Epilogue operands of one (row, column-chunk), loaded ahead of the row's gathers so
+// their latency overlaps them (fields an op does not use are optimised away).
+template <class T, int KV>
+struct PreT {
+  T x[KV];
+  T b[KV];
+  T c[KV];
+  T d;
+};
+
 struct RedCtx {
   double* partials;    // [gridDim.x * k]
   unsigned* counter;   // ticket counter, left at 0 after every kernel
   int k;
 };
 
-// Sum each column's CTA partials in a fixed order in the last CTA, then call
+constexpr int kRedGroups = 16;  // first-level groups of CTAs in the grid reduction
+
+// Sum nparts partial rows (stride k) for every column with all threads of the CTA; the
+// per-column order is fixed (deterministic).  Thread (slice sl, column ci) strides over
+// parts; slices are combined by a shared-memory tree.  Results for columns cb..cb+kc
+// land in sbuf[0..kc).
+__device__ __forceinline__ void sum_parts(const double* parts, int nparts, int k, int cb, int kc,
+                                          double* sbuf) {
+  const int nsl = kBlock / kc;
+  const int ci = threadIdx.x % kc, sl = threadIdx.x / kc;
+  const int c = cb + ci;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  if (c < k) {
+    int b = sl;
+    for (; b + 3 * nsl < nparts; b += 4 * nsl) {
+      a0 += __ldcg(parts + (size_t)b * k + c);
+      a1 += __ldcg(parts + (size_t)(b + nsl) * k + c);
+      a2 += __ldcg(parts + (size_t)(b + 2 * nsl) * k + c);
+      a3 += __ldcg(parts + (size_t)(b + 3 * nsl) * k + c);
+    }
+    for (; b < nparts; b += nsl) a0 += __ldcg(parts + (size_t)b * k + c);
+  }
+  sbuf[threadIdx.x] = (a0 + a1) + (a2 + a3);
+  __syncthreads();
+  for (int st = nsl >> 1; st > 0; st >>= 1) {
+    if (sl < st) sbuf[sl * kc + ci] += sbuf[(sl + st) * kc + ci];
+    __syncthreads();
+  }
+}
+
+// Grid reduction, two levels, deterministic: CTAs are split into kRedGroups contiguous
+// groups; the last CTA of a group (ticket counter) sums the group's partials into a
+// group row; the last group to finish sums the group rows, then calls
 // op.finalize_col(c, sum) for every column and op.finalize_all(any) once.
+// partials: [gridDim.x][k] CTA rows followed by [kRedGroups][k] group rows;
+// counter: [0] groups done, [1 + g] CTAs done in group g (all left at 0).
 template <class Op>
 __device__ __forceinline__ void grid_finish(const Op& op, const RedCtx& rc, double* sbuf) {
   __shared__ unsigned s_last;
+  const int k = rc.k;
+  const int nb = gridDim.x;
+  const int ng = nb < kRedGroups ? nb : kRedGroups;
+  const int gsz = (nb + ng - 1) / ng;
+  const int g = blockIdx.x / gsz;
+  const int g0 = g * gsz;
+  const int gn = min(gsz, nb - g0);
+  const int ngroups = (nb + gsz - 1) / gsz;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(rc.counter, 1u) == gridDim.x - 1) ? 1u : 0u;
+  if (threadIdx.x == 0) s_last = (atomicAdd(rc.counter + 1 + g, 1u) == (unsigned)(gn - 1)) ? 1u : 0u;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  const int k = rc.k;
   int kc = 1;
   while (kc < k && kc < kBlock) kc <<= 1;
-  const int nsl = kBlock / kc;
-  const int ci = threadIdx.x % kc, sl = threadIdx.x / kc;
+  double* grow = rc.partials + (size_t)nb * k;
+  for (int cb = 0; cb < k; cb += kc) {
+    sum_parts(rc.partials + (size_t)g0 * k, gn, k, cb, kc, sbuf);
+    if (threadIdx.x < kc && cb + threadIdx.x < k) grow[(size_t)g * k + cb + threadIdx.x] = sbuf[threadIdx.x];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) rc.counter[1 + g] = 0u;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(rc.counter, 1u) == (unsigned)(ngroups - 1)) ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
   int any = 0;
   for (int cb = 0; cb < k; cb += kc) {
-    const int c = cb + ci;
-    double s = 0.0;
-    if (c < k)
-      for (int b = sl; b < (int)gridDim.x; b += nsl) s += __ldcg(rc.partials + (size_t)b * k + c);
-    sbuf[threadIdx.x] = s;
-    __syncthreads();
-    for (int st = nsl >> 1; st > 0; st >>= 1) {
-      if (sl < st) sbuf[sl * kc + ci] += sbuf[(sl + st) * kc + ci];
-      __syncthreads();
-    }
-    if (sl == 0 && c < k) any |= op.finalize_col(c, sbuf[ci]);
+    sum_parts(grow, ngroups, k, cb, kc, sbuf);
+    if (threadIdx.x < kc && cb + threadIdx.x < k) any |= op.finalize_col(cb + threadIdx.x, sbuf[threadIdx.x]);
     __syncthreads();
   }
   any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
     op.finalize_all(any);
-    *rc.counter = 0u;
+    rc.counter[0] = 0u;
   }
 }
 
@@ -137,15 +197,15 @@ __device__ __forceinline__ void block_reduce_1(const Op& op, const RedCtx& rc, d
 }
 
 // CTA-level reduction for k > 1: thread (grp, lane) owns columns (lane + j*G)*KV + v.
-template <class Op, int G, int KV>
+template <class Op, int G, int KV, int NCH>
 __device__ __forceinline__ void block_reduce_k(const Op& op, const RedCtx& rc,
-                                               const double (&red)[kMaxCh][KV]) {
+                                               const double (&red)[NCH][KV]) {
   extern __shared__ double dyn[];   // (kBlock / G) * k doubles
   const int k = rc.k;
   const int lane = threadIdx.x % G, grp = threadIdx.x / G;
   const int nchunks = k / KV;
 #pragma unroll
-  for (int j = 0; j < kMaxCh; ++j) {
+  for (int j = 0; j < NCH; ++j) {
     const int ch = lane + j * G;
     if (ch < nchunks) {
 #pragma unroll
@@ -192,50 +252,122 @@ csr_k1(const int* __restrict__ rowptr, const int* __restrict__ col,
   if (op.reduces()) block_reduce_1(op, rc, red);
 }
 
-// k > 1: G lanes per row split the columns in KV-wide vectors.
-template <class Op, int G, int KV>
-__global__ void __launch_bounds__(kBlock)
+// k > 1: G lanes per row split the columns in KV-wide vectors (NCH chunks per lane).
+// Latency hiding, per row: the G lanes load up to G of the row's (col, val) pairs in one
+// coalesced access and broadcast them with shuffles; the gathered x rows are issued up
+// to 8 at a time as independent loads, together with the row's epilogue operands and the
+// next row's row pointers; the next row's (col, val) are fetched before this row's
+// arithmetic, so one memory round trip per row remains exposed instead of five.
+template <class Op, int G, int KV, int NCH>
+__global__ void __launch_bounds__(kBlock, 4)
 csr_kb(const int* __restrict__ rowptr, const int* __restrict__ col,
        const typename Op::V* __restrict__ val, int n_rows, Op op, RedCtx rc) {
   count_launch();
   if (op.stopped()) return;
   using A = typename Op::Acc;
+  // gathered x rows in flight per batch: 16-byte vectors 4 at a time, narrower ones 8
+  constexpr int kB = (sizeof(A) * KV >= 16) ? 4 : 8;
   const int k = rc.k;
   const int lane = threadIdx.x % G;
   const int grp = (blockIdx.x * kBlock + threadIdx.x) / G;
   const int ngrp = gridDim.x * (kBlock / G);
   const int nchunks = k / KV;
-  double red[kMaxCh][KV];
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+  double red[NCH][KV];
 #pragma unroll
-  for (int j = 0; j < kMaxCh; ++j)
+  for (int j = 0; j < NCH; ++j)
 #pragma unroll
     for (int v = 0; v < KV; ++v) red[j][v] = 0.0;
-  for (int row = grp; row < n_rows; row += ngrp) {
-    const int s = __ldg(rowptr + row), e = __ldg(rowptr + row + 1);
-#pragma unroll
-    for (int j = 0; j < kMaxCh; ++j) {
-      const int ch = lane + j * G;
-      if (ch < nchunks) {
-        A acc[KV];
-#pragma unroll
-        for (int v = 0; v < KV; ++v) acc[v] = A(0);
-        for (int nz = s; nz < e; ++nz) {
-          const A a = static_cast<A>(__ldg(val + nz));
-          A xv[KV];
-          op.template xk<KV>(__ldg(col + nz), ch * KV, xv);
-#pragma unroll
-          for (int v = 0; v < KV; ++v) acc[v] += a * xv[v];
-        }
-        op.template epik<KV>(row, ch * KV, acc, red[j]);
-      }
+  int row = grp;
+  int s = 0, e = 0, c_l = 0;
+  A v_l = A(0);
+  if (row < n_rows) {
+    s = __ldg(rowptr + row);
+    e = __ldg(rowptr + row + 1);
+    if (s + lane < e) {
+      c_l = __ldg(col + s + lane);
+      v_l = static_cast<A>(__ldg(val + s + lane));
     }
   }
-  if (op.reduces()) block_reduce_k<Op, G, KV>(op, rc, red);
+  for (; row < n_rows; row += ngrp) {
+    const int nrow = row + ngrp;
+    int ns = 0, ne = 0;
+    if (nrow < n_rows) {
+      ns = __ldg(rowptr + nrow);
+      ne = __ldg(rowptr + nrow + 1);
+    }
+    PreT<A, KV> pre[NCH];
+#pragma unroll
+    for (int j = 0; j < NCH; ++j)
+      if (lane + j * G < nchunks) op.template prek<KV>(row, (lane + j * G) * KV, pre[j]);
+    A acc[NCH][KV];
+#pragma unroll
+    for (int j = 0; j < NCH; ++j)
+#pragma unroll
+      for (int v = 0; v < KV; ++v) acc[j][v] = A(0);
+    for (int base = s; base < e; base += G) {
+      if (base != s) {  // rows longer than G: next chunk of (col, val)
+        c_l = 0;
+        v_l = A(0);
+        if (base + lane < e) {
+          c_l = __ldg(col + base + lane);
+          v_l = static_cast<A>(__ldg(val + base + lane));
+        }
+      }
+      const int cnt = min(G, e - base);
+      for (int t = 0; t < cnt; t += kB) {
+        int cc[kB];
+        A vv[kB];
+#pragma unroll
+        for (int u = 0; u < kB; ++u) {
+          const int src = (t + u < G) ? t + u : 0;
+          cc[u] = __shfl_sync(gmask, c_l, src, G);
+          vv[u] = __shfl_sync(gmask, v_l, src, G);
+          if (t + u >= cnt) vv[u] = A(0);
+        }
+#pragma unroll
+        for (int j = 0; j < NCH; ++j) {
+          const int ch = lane + j * G;
+          if (ch < nchunks) {
+            A xv[kB][KV];
+#pragma unroll
+            for (int u = 0; u < kB; ++u) {
+              if (t + u < cnt) {
+                op.template xk<KV>(cc[u], ch * KV, xv[u]);
+              } else {
+#pragma unroll
+                for (int v = 0; v < KV; ++v) xv[u][v] = A(0);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < kB; ++u)
+#pragma unroll
+              for (int v = 0; v < KV; ++v) acc[j][v] += vv[u] * xv[u][v];
+          }
+        }
+      }
+    }
+    // next row's first (col, val) chunk, issued before this row's epilogue
+    s = ns;
+    e = ne;
+    c_l = 0;
+    v_l = A(0);
+    if (s + lane < e) {
+      c_l = __ldg(col + s + lane);
+      v_l = static_cast<A>(__ldg(val + s + lane));
+    }
+#pragma unroll
+    for (int j = 0; j < NCH; ++j) {
+      const int ch = lane + j * G;
+      if (ch < nchunks) op.template epik<KV>(row, ch * KV, acc[j], pre[j], red[j]);
+    }
+  }
+  if (op.reduces()) block_reduce_k<Op, G, KV, NCH>(op, rc, red);
 }
 
-// Elementwise over [n_rows, k] with the same (group, lane, KV) mapping.
-template <class Op, int G, int KV>
-__global__ void __launch_bounds__(kBlock)
+// Elementwise over [n_rows, k] with the same (group, lane, KV, NCH) mapping.
+template <class Op, int G, int KV, int NCH>
+__global__ void __launch_bounds__(kBlock, 4)
 elem_kb(int n_rows, Op op, RedCtx rc) {
   count_launch();
   if (op.stopped()) return;
@@ -244,14 +376,14 @@ elem_kb(int n_rows, Op op, RedCtx rc) {
   const int grp = (blockIdx.x * kBlock + threadIdx.x) / G;
   const int ngrp = gridDim.x * (kBlock / G);
   const int nchunks = k / KV;
-  double red[kMaxCh][KV];
+  double red[NCH][KV];
 #pragma unroll
-  for (int j = 0; j < kMaxCh; ++j)
+  for (int j = 0; j < NCH; ++j)
 #pragma unroll
     for (int v = 0; v < KV; ++v) red[j][v] = 0.0;
   for (int row = grp; row < n_rows; row += ngrp) {
 #pragma unroll
-    for (int j = 0; j < kMaxCh; ++j) {
+    for (int j = 0; j < NCH; ++j) {
       const int ch = lane + j * G;
       if (ch < nchunks) op.template elem<KV>(row, ch * KV, red[j]);
     }
@@ -260,7 +392,7 @@ elem_kb(int n_rows, Op op, RedCtx rc) {
     if (k == 1) {
       block_reduce_1(op, rc, red[0][0]);
     } else {
-      block_reduce_k<Op, G, KV>(op, rc, red);
+      block_reduce_k<Op, G, KV, NCH>(op, rc, red);
     }
   }
 }
@@ -382,16 +514,21 @@ struct OpJacobi {
     return 0.0;
   }
   template <int KV>
-  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], double (&red)[KV]) const {
-    T xv[KV], bv[KV], y[KV], r[KV];
-    xs.template getk<KV>(i, c0, xv);
-    ld_vec<T, KV>(b + (size_t)i * ld + c0, bv);
-    const T d = __ldg(dinv + i);
+  __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& p) const {
+    const size_t o = (size_t)i * ld + c0;
+    xs.template getk<KV>(i, c0, p.x);
+    ld_vec<T, KV>(b + o, p.b);
+    p.d = __ldg(dinv + i);
+  }
+  template <int KV>
+  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& p,
+                                       double (&red)[KV]) const {
+    T y[KV], r[KV];
 #pragma unroll
     for (int v = 0; v < KV; ++v) {
-      r[v] = bv[v] - s[v];
-      const T temp = d * r[v] + xv[v];
-      y[v] = (T(1) - omega) * xv[v] + omega * temp;
+      r[v] = p.b[v] - s[v];
+      const T temp = p.d * r[v] + p.x[v];
+      y[v] = (T(1) - omega) * p.x[v] + omega * temp;
     }
     const size_t o = (size_t)i * ld + c0;
     if (norm) {
@@ -455,12 +592,16 @@ struct OpResid {
     return NORM ? (double)r * (double)r : 0.0;
   }
   template <int KV>
-  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], double (&red)[KV]) const {
-    T bv[KV], r[KV];
-    ld_vec<T, KV>(b + (size_t)i * ld + c0, bv);
+  __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& p) const {
+    ld_vec<T, KV>(b + (size_t)i * ld + c0, p.b);
+  }
+  template <int KV>
+  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& p,
+                                       double (&red)[KV]) const {
+    T r[KV];
 #pragma unroll
     for (int v = 0; v < KV; ++v) {
-      r[v] = bv[v] - s[v];
+      r[v] = p.b[v] - s[v];
       if constexpr (NORM) red[v] += (double)r[v] * (double)r[v];
     }
     if constexpr (STORE) st_vec<T, KV>(out + (size_t)i * ld + c0, r);
@@ -506,12 +647,16 @@ struct OpAxpy {
     return 0.0;
   }
   template <int KV>
-  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], double (&)[KV]) const {
-    T bv[KV];
-    base.template getk<KV>(i, c0, bv);
+  __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& p) const {
+    base.template getk<KV>(i, c0, p.x);
+  }
+  template <int KV>
+  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& p,
+                                       double (&)[KV]) const {
+    T y[KV];
 #pragma unroll
-    for (int v = 0; v < KV; ++v) bv[v] += s[v];
-    st_vec<T, KV>(out + (size_t)i * ld + c0, bv);
+    for (int v = 0; v < KV; ++v) y[v] = p.x[v] + s[v];
+    st_vec<T, KV>(out + (size_t)i * ld + c0, y);
   }
   __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
   __device__ __forceinline__ void finalize_all(int) const {}
@@ -538,22 +683,101 @@ struct OpCgQ {
     ld_vec<T, KV>(p + (size_t)j * ld + c0, v);
   }
   __device__ __forceinline__ double epi1(int i, T s) const {
-    q[i] = s;
+    if (q) q[i] = s;
     return (double)__ldg(p + i) * (double)s;
   }
   template <int KV>
-  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], double (&red)[KV]) const {
-    T pv[KV];
-    ld_vec<T, KV>(p + (size_t)i * ld + c0, pv);
+  __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
+    ld_vec<T, KV>(p + (size_t)i * ld + c0, pp.x);
+  }
+  template <int KV>
+  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& pp,
+                                       double (&red)[KV]) const {
 #pragma unroll
-    for (int v = 0; v < KV; ++v) red[v] += (double)pv[v] * (double)s[v];
-    st_vec<T, KV>(q + (size_t)i * ld + c0, s);
+    for (int v = 0; v < KV; ++v) red[v] += (double)pp.x[v] * (double)s[v];
+    if (q) st_vec<T, KV>(q + (size_t)i * ld + c0, s);
   }
   __device__ __forceinline__ int finalize_col(int c, double s) const {
     alpha[c] = gamma[c] / s;
     return 1;
   }
   __device__ __forceinline__ void finalize_all(int) const {}
+};
+
+// CG update with the SpMV recomputed instead of stored: s = A p, then for active columns
+// x += alpha p, r -= alpha s; r copied into the cycle's type (r_lo, nullable); reduce
+// <r, r> and apply the CG loop rule.
+template <class T, class TLO>
+struct OpCgUpdA {
+  using V = T;
+  using Acc = T;
+  static constexpr bool kReduce = true;
+  __host__ __device__ __forceinline__ bool reduces() const { return kReduce; }
+  T* x;
+  T* r;
+  const T* p;
+  TLO* r_lo;
+  const double* alpha;
+  const int* active;
+  int ld;
+  const int* stop;
+  LoopCtl ctl;
+
+  __device__ __forceinline__ bool stopped() const { return stop && *stop; }
+  __device__ __forceinline__ T x1(int j) const { return __ldg(p + j); }
+  template <int KV>
+  __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const {
+    ld_vec<T, KV>(p + (size_t)j * ld + c0, v);
+  }
+  __device__ __forceinline__ double epi1(int i, T s) const {
+    T rv = r[i];
+    if (active[0]) {
+      const T a = static_cast<T>(alpha[0]);
+      x[i] = x[i] + a * __ldg(p + i);
+      rv = rv - a * s;
+      r[i] = rv;
+    }
+    if (r_lo) r_lo[i] = static_cast<TLO>(rv);
+    return (double)rv * (double)rv;
+  }
+  template <int KV>
+  __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
+    const size_t o = (size_t)i * ld + c0;
+    ld_vec<T, KV>(p + o, pp.x);
+    ld_vec<T, KV>(x + o, pp.b);
+    ld_vec<T, KV>(r + o, pp.c);
+  }
+  template <int KV>
+  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& pp,
+                                       double (&red)[KV]) const {
+    const size_t o = (size_t)i * ld + c0;
+    T xv[KV], rv[KV];
+    bool any = false;
+#pragma unroll
+    for (int v = 0; v < KV; ++v) {
+      xv[v] = pp.b[v];
+      rv[v] = pp.c[v];
+      if (active[c0 + v]) {
+        const T a = static_cast<T>(alpha[c0 + v]);
+        xv[v] = xv[v] + a * pp.x[v];
+        rv[v] = rv[v] - a * s[v];
+        any = true;
+      }
+      red[v] += (double)rv[v] * (double)rv[v];
+    }
+    if (any) {
+      st_vec<T, KV>(x + o, xv);
+      st_vec<T, KV>(r + o, rv);
+    }
+    if (r_lo) {
+      TLO rl[KV];
+#pragma unroll
+      for (int v = 0; v < KV; ++v) rl[v] = static_cast<TLO>(rv[v]);
+      st_vec<TLO, KV>(r_lo + o, rl);
+    }
+  }
+  __device__ __forceinline__ int finalize_col(int c, double s) const { return ctl.cg_col(c, s); }
+  __device__ __forceinline__ void finalize_all(int any) const { ctl.set_any(any); }
 };
 
 // ------------------------------------------------------------------ elementwise ops

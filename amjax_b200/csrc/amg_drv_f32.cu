@@ -52,13 +52,15 @@ void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     run_elem<TC>(n0, cp, q.k, red_of(pl), cs, {z, p});
   };
   auto body = [&](cudaStream_t cs) {
-    OpCgQ<TO> qop{p, qv, q.k, pl->stop(), pl->gamma(), pl->alpha()};
-    run_csr(*A0, qop, q.k, red_of(pl), cs, {p, qv});
-    OpCgUpdate<TO, TC> up{};
-    up.x = x; up.r = r; up.p = p; up.q = qv; up.r_lo = mixed ? rc : nullptr;
+    // <p, A p> only (A p is recomputed in the update instead of stored)
+    OpCgQ<TO> qop{p, nullptr, q.k, pl->stop(), pl->gamma(), pl->alpha()};
+    run_csr(*A0, qop, q.k, red_of(pl), cs, {p});
+    OpCgUpdA<TO, TC> up{};
+    up.x = x; up.r = r; up.p = p; up.r_lo = mixed ? rc : nullptr;
     up.alpha = pl->alpha(); up.active = pl->active(); up.ld = q.k; up.stop = pl->stop();
     up.ctl = make_ctl(pl, q.maxiter);
-    run_elem<TC>(n0, up, q.k, red_of(pl), cs, {x, r, p, qv, up.r_lo});
+    run_csr(*A0, up, q.k, red_of(pl), cs, {x, r, p, up.r_lo});
+    (void)qv;
     cycle(cs);
     OpCgDir<TO, TC> dir{p, z, pl->beta(), q.k, pl->stop()};
     run_elem<TC>(n0, dir, q.k, red_of(pl), cs, {p, z});

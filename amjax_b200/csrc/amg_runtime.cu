@@ -30,6 +30,28 @@ DevInfo dev_info() {
   return d;
 }
 
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("AMG_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+int resident_ctas(const void* fn, size_t smem) {
+  static std::mutex m;
+  static std::map<std::pair<const void*, size_t>, int> cache;
+  std::lock_guard<std::mutex> lk(m);
+  auto key = std::make_pair(fn, smem);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int nb = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kBlock, smem));
+  nb = std::max(1, std::min(nb, 2048 / kBlock));
+  cache[key] = nb;
+  return nb;
+}
+
 void check_csr(const amg_csr& c, const char* what, int lvl) {
   if (c.n_rows < 0 || c.n_cols < 0 || c.nnz < 0)
     fail(AMG_ERR_INVALID_ARG, "level %d %s: negative size", lvl, what);
@@ -94,9 +116,10 @@ Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s) {
   pl->dscal = static_cast<double*>(pl->alloc(sizeof(double) * 6 * k));
   pl->iscal = static_cast<int*>(pl->alloc(sizeof(int) * (2 * k + 2)));
   CK(cudaMemset(pl->iscal, 0, sizeof(int) * (2 * k + 2)));
-  pl->partials = static_cast<double*>(pl->alloc(sizeof(double) * size_t(dev_info().max_ctas) * k));
-  pl->counter = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * 4));
-  CK(cudaMemset(pl->counter, 0, sizeof(unsigned) * 4));
+  pl->partials = static_cast<double*>(
+      pl->alloc(sizeof(double) * size_t(dev_info().max_ctas + kRedGroups) * k));
+  pl->counter = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * (1 + kRedGroups)));
+  CK(cudaMemset(pl->counter, 0, sizeof(unsigned) * (1 + kRedGroups)));
   CK(cudaHostAlloc(reinterpret_cast<void**>(&pl->h_stop), sizeof(int), cudaHostAllocDefault));
   Plan* raw = pl.get();
   h->plans[key] = std::move(pl);
@@ -173,7 +196,7 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
     if (has_loop) {
       for (int trip = 0;; ++trip) {
         body(user);
-        loop_guard_host_kernel<<<1, 32, 0, user>>>(pl->stop(), pl->gcount(), gmax);
+        launch(loop_guard_host_kernel, 1, 32, 0, user, pl->stop(), pl->gcount(), gmax);
         CK_LAUNCH();
         CK(cudaMemcpyAsync(pl->h_stop, pl->stop(), sizeof(int), cudaMemcpyDeviceToHost, user));
         CK(cudaStreamSynchronize(user));
@@ -215,7 +238,7 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
         int* gc = pl->gcount();
         capture(bg, nullptr, 0, [&](cudaStream_t cs) {
           body(cs);
-          loop_guard_kernel<<<1, 32, 0, cs>>>(stp, gc, gmax, hc);
+          launch(loop_guard_kernel, 1, 32, 0, cs, stp, gc, gmax, hc);
           CK_LAUNCH();
         });
         pl->nodes_body = count_nodes(bg);
@@ -238,7 +261,7 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
       int* gc = pl->gcount();
       capture(bg, nullptr, 0, [&](cudaStream_t cs) {
         body(cs);
-        loop_guard_host_kernel<<<1, 32, 0, cs>>>(stp, gc, gmax);
+        launch(loop_guard_host_kernel, 1, 32, 0, cs, stp, gc, gmax);
         CK_LAUNCH();
       });
       CK(cudaGraphInstantiate(&e->body_exec, bg, 0));

@@ -216,7 +216,7 @@ namespace amg {
 
 // ------------------------------------------------------------------ launch helpers
 struct Cfg {
-  int G = 1, KV = 1, grid = 1;
+  int G = 1, KV = 1, NCH = 1, grid = 1;
   size_t smem = 0;
 };
 
@@ -247,8 +247,10 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     c.KV = pick_kv<T>(k, ptrs);
     const int nch = k / c.KV;
     c.G = std::max(4, std::min(32, pow2ceil(nch)));
-    if ((nch + c.G - 1) / c.G > kMaxCh)
+    const int per = (nch + c.G - 1) / c.G;
+    if (per > kMaxCh)
       fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);
+    c.NCH = per <= 1 ? 1 : per <= 2 ? 2 : 4;
     c.smem = sizeof(double) * std::max<size_t>(size_t(kBlock / c.G) * k, kBlock);
   }
   const int rows_per_cta = kBlock / c.G;
@@ -262,26 +264,62 @@ struct Red {
   unsigned* counter = nullptr;
 };
 
+// Launch with programmatic stream serialization (PDL): the kernel may start while its
+// predecessor on the stream drains; every kernel of this library begins with
+// griddepcontrol.wait, so correctness does not depend on it.  AMG_PDL=0 disables.
+bool pdl_enabled();
+
+template <class... Exp, class... Act>
+static void launch(void (*kernel)(Exp...), int grid, int block, size_t smem, cudaStream_t s,
+                   Act&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  CK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...));
+}
+
+// Resident CTAs per SM of one kernel instantiation (cached): grids are capped at
+// SMs x this, so a grid-stride kernel runs in a single wave.
+int resident_ctas(const void* fn, size_t smem);
+
+template <class K>
+static int cap_grid(K* fn, int grid, size_t smem) {
+  const int per_sm = resident_ctas(reinterpret_cast<const void*>(fn), smem);
+  return std::max(1, std::min(grid, dev_info().nsm * per_sm));
+}
+
 template <class Op, int G>
 static void launch_k1(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                       RedCtx rc, cudaStream_t s) {
-  csr_k1<Op, G><<<c.grid, kBlock, 0, s>>>(M.rowptr, M.col, vals, M.n_rows, op, rc);
+  const int grid = cap_grid(csr_k1<Op, G>, c.grid, 0);
+  launch(csr_k1<Op, G>, grid, kBlock, 0, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
 }
 
-template <class Op, int G, int KV>
+template <class Op, int G, int KV, int NCH>
 static void launch_kb(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                       RedCtx rc, cudaStream_t s) {
-  csr_kb<Op, G, KV><<<c.grid, kBlock, c.smem, s>>>(M.rowptr, M.col, vals, M.n_rows, op, rc);
+  const int grid = cap_grid(csr_kb<Op, G, KV, NCH>, c.grid, c.smem);
+  launch(csr_kb<Op, G, KV, NCH>, grid, kBlock, c.smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
 }
 
+// (G, NCH) pairs: NCH = 1 for any G; NCH > 1 only with G = 32.
 template <class Op, int KV>
 static void dispatch_kb_g(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                           RedCtx rc, cudaStream_t s) {
+  if (c.NCH == 2) { launch_kb<Op, 32, KV, 2>(M, vals, op, c, rc, s); return; }
+  if (c.NCH == 4) { launch_kb<Op, 32, KV, 4>(M, vals, op, c, rc, s); return; }
   switch (c.G) {
-    case 4: launch_kb<Op, 4, KV>(M, vals, op, c, rc, s); break;
-    case 8: launch_kb<Op, 8, KV>(M, vals, op, c, rc, s); break;
-    case 16: launch_kb<Op, 16, KV>(M, vals, op, c, rc, s); break;
-    default: launch_kb<Op, 32, KV>(M, vals, op, c, rc, s); break;
+    case 4: launch_kb<Op, 4, KV, 1>(M, vals, op, c, rc, s); break;
+    case 8: launch_kb<Op, 8, KV, 1>(M, vals, op, c, rc, s); break;
+    case 16: launch_kb<Op, 16, KV, 1>(M, vals, op, c, rc, s); break;
+    default: launch_kb<Op, 32, KV, 1>(M, vals, op, c, rc, s); break;
   }
 }
 
@@ -305,28 +343,30 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
       default: launch_k1<Op, 32>(M, vals, op, c, rc, s); break;
     }
   } else {
-    switch (c.KV) {
-      case 1: dispatch_kb_g<Op, 1>(M, vals, op, c, rc, s); break;
-      case 2: dispatch_kb_g<Op, 2>(M, vals, op, c, rc, s); break;
-      default: dispatch_kb_g<Op, 4>(M, vals, op, c, rc, s); break;
-    }
+    if (c.KV == 1) dispatch_kb_g<Op, 1>(M, vals, op, c, rc, s);
+    else if (c.KV == 2) dispatch_kb_g<Op, 2>(M, vals, op, c, rc, s);
+    else if constexpr (sizeof(typename Op::Acc) == 4) dispatch_kb_g<Op, 4>(M, vals, op, c, rc, s);
+    else fail(AMG_ERR_INVALID_ARG, "internal: 4-wide FP64 vectors");
   }
   CK_LAUNCH();
 }
 
-template <class Op, int G, int KV>
+template <class Op, int G, int KV, int NCH>
 static void launch_elem(int n, const Op& op, const Cfg& c, RedCtx rc, cudaStream_t s) {
-  elem_kb<Op, G, KV><<<c.grid, kBlock, c.smem, s>>>(n, op, rc);
+  const int grid = cap_grid(elem_kb<Op, G, KV, NCH>, c.grid, c.smem);
+  launch(elem_kb<Op, G, KV, NCH>, grid, kBlock, c.smem, s, n, op, rc);
 }
 
 template <class Op, int KV>
 static void dispatch_elem_g(int n, const Op& op, const Cfg& c, RedCtx rc, cudaStream_t s) {
+  if (c.NCH == 2) { launch_elem<Op, 32, KV, 2>(n, op, c, rc, s); return; }
+  if (c.NCH == 4) { launch_elem<Op, 32, KV, 4>(n, op, c, rc, s); return; }
   switch (c.G) {
-    case 1: launch_elem<Op, 1, KV>(n, op, c, rc, s); break;
-    case 4: launch_elem<Op, 4, KV>(n, op, c, rc, s); break;
-    case 8: launch_elem<Op, 8, KV>(n, op, c, rc, s); break;
-    case 16: launch_elem<Op, 16, KV>(n, op, c, rc, s); break;
-    default: launch_elem<Op, 32, KV>(n, op, c, rc, s); break;
+    case 1: launch_elem<Op, 1, KV, 1>(n, op, c, rc, s); break;
+    case 4: launch_elem<Op, 4, KV, 1>(n, op, c, rc, s); break;
+    case 8: launch_elem<Op, 8, KV, 1>(n, op, c, rc, s); break;
+    case 16: launch_elem<Op, 16, KV, 1>(n, op, c, rc, s); break;
+    default: launch_elem<Op, 32, KV, 1>(n, op, c, rc, s); break;
   }
 }
 
@@ -343,11 +383,10 @@ static void run_elem(int n, const Op& op, int k, const Red& red, cudaStream_t s,
   }
   RedCtx rc{red.partials, red.counter, k};
   if (op.reduces() && !red.partials) fail(AMG_ERR_INVALID_ARG, "reduction scratch missing");
-  switch (c.KV) {
-    case 1: dispatch_elem_g<Op, 1>(n, op, c, rc, s); break;
-    case 2: dispatch_elem_g<Op, 2>(n, op, c, rc, s); break;
-    default: dispatch_elem_g<Op, 4>(n, op, c, rc, s); break;
-  }
+  if (c.KV == 1) dispatch_elem_g<Op, 1>(n, op, c, rc, s);
+  else if (c.KV == 2) dispatch_elem_g<Op, 2>(n, op, c, rc, s);
+  else if constexpr (sizeof(TA) == 4) dispatch_elem_g<Op, 4>(n, op, c, rc, s);
+  else fail(AMG_ERR_INVALID_ARG, "internal: 4-wide FP64 vectors");
   CK_LAUNCH();
 }
 
@@ -507,13 +546,12 @@ struct Cycle {
     const int tot = n * k;
     const int grid = std::max(1, std::min((tot + 127) / 128, dev_info().max_ctas));
     if (c.kind == AMG_COARSE_PINV) {
-      coarse_gemv<T><<<grid, 128, 0, s>>>(c.template m0<T>(), b, x, n, k, 0, stop);
+      launch(coarse_gemv<T>, grid, 128, 0, s, c.template m0<T>(), (const T*)b, x, n, k, 0, stop);
     } else if (c.kind == AMG_COARSE_LU) {
-      coarse_trsv<T, 0><<<(k + 63) / 64, 64, 0, s>>>(c.template m0<T>(), c.perm, b, x, n, k, stop);
+      launch(coarse_trsv<T, 0>, (k + 63) / 64, 64, 0, s, c.template m0<T>(), c.perm, (const T*)b, x, n, k, stop);
     } else if (c.kind == AMG_COARSE_QR) {
-      coarse_gemv<T><<<grid, 128, 0, s>>>(c.template m0<T>(), b, x, n, k, 1, stop);
-      CK_LAUNCH();
-      coarse_trsv<T, 1><<<(k + 63) / 64, 64, 0, s>>>(c.template m1<T>(), nullptr, x, x, n, k, stop);
+      launch(coarse_gemv<T>, grid, 128, 0, s, c.template m0<T>(), (const T*)b, x, n, k, 1, stop);
+      launch(coarse_trsv<T, 1>, (k + 63) / 64, 64, 0, s, c.template m1<T>(), (const int*)nullptr, (const T*)x, x, n, k, stop);
     } else {  // Jacobi sweeps from zero on the coarsest operator
       const T om = T(c.omega);
       // level l's own right-hand side buffer is b (== B[l]); sweeps read Bb(l)

@@ -264,7 +264,11 @@ class MultilevelSolver:
             if t.dim() > 1 and t.shape[0] != n:
                 t = t.reshape(-1)
             if not on_dev:
-                t = t.to(dtype).pin_memory().to(dev, non_blocking=True)
+                if t.dtype != dtype:
+                    t = t.to(dtype)
+                if not t.is_pinned():
+                    t = t.pin_memory()
+                t = t.to(dev, non_blocking=True)
             t = t.to(device=dev, dtype=dtype).contiguous()
             if t.dim() == 1 and t.numel() != n:
                 raise ValueError(f"b has {t.numel()} entries, expected {n}")
@@ -288,7 +292,7 @@ class MultilevelSolver:
 
     # ------------------------------------------------------------------ solve
     def solve(self, b, A=None, x0=None, tol=1e-5, maxiter=100, cycle="V", cycles_per_level=1,
-              precision=None, return_info=False):
+              precision=None, return_info=False, out=None):
         """Solve A x = b by repeated cycles (multilevel.py:341-425).
 
         Stops per column when ``||b - A x|| < tol ||b||`` or after ``maxiter`` cycles
@@ -313,8 +317,8 @@ class MultilevelSolver:
         x, info = self._solve_dev(bd, A0, tol, maxiter, cycle, cycles_per_level, prec)
         if x0 is not None:
             x = x + x0d
-        out = back(x)
-        return (out, info) if return_info else out
+        res = _deliver(x, back, out)
+        return (res, info) if return_info else res
 
     def _solve_dev(self, bd, A0, tol, maxiter, cycle, cycles_per_level, prec):
         h = self._native()
@@ -329,7 +333,7 @@ class MultilevelSolver:
         return x, info
 
     def pcg(self, b, A=None, x0=None, tol=1e-5, atol=0.0, maxiter=None, cycle="V", cycles_per_level=1,
-            precision=None, return_info=False):
+            precision=None, return_info=False, out=None):
         """CG preconditioned by one cycle, fused on the device: the same iteration as
         ``jax.scipy.sparse.linalg.cg(A, b, M=ml.aspreconditioner(cycle))`` (stop when
         ``<r,r> <= max(tol^2 <b,b>, atol^2)``, default ``maxiter = 10 N``)."""
@@ -350,8 +354,8 @@ class MultilevelSolver:
         x, info = self._pcg_dev(bd, A0, tol, atol, maxiter, cycle, cycles_per_level, prec)
         if x0 is not None:
             x = x + x0d
-        out = back(x)
-        return (out, info) if return_info else out
+        res = _deliver(x, back, out)
+        return (res, info) if return_info else res
 
     def _pcg_dev(self, bd, A0, tol, atol, maxiter, cycle, cycles_per_level, prec):
         h = self._native()
@@ -427,6 +431,16 @@ class MultilevelSolver:
         mt._transposed = self
         self._transposed = mt
         return mt
+
+
+def _deliver(x, back, out):
+    """Return the device result in the caller's kind, or copy it into ``out`` (a
+    preallocated tensor, e.g. pinned host memory: the copy is then asynchronous on the
+    current stream and complete once that stream is synchronised)."""
+    if out is None:
+        return back(x)
+    out.copy_(x.reshape(out.shape), non_blocking=True)
+    return out
 
 
 def _hierarchy_symmetric(ml) -> bool:
