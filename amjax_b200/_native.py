@@ -57,6 +57,8 @@ SIGNATURES = {
                           C.POINTER(C.c_double), C.c_void_p]),
     "amg_jacobi": (C.c_int, [C.POINTER(amg_csr), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_int32, C.c_int32, C.c_double, C.c_void_p]),
+    "amg_jacobi_noalloc": (C.c_int, [C.POINTER(amg_csr), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_void_p]),
     "amg_spmv": (C.c_int, [C.POINTER(amg_csr), C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "amg_inverse_diagonal": (C.c_int, [C.POINTER(amg_csr), C.c_int32, C.c_void_p, C.c_void_p]),
     "amg_sampled_outer": (C.c_int, [C.POINTER(amg_csr), C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,

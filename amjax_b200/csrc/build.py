@@ -19,7 +19,8 @@ PKG = HERE.parent
 ROOT = PKG.parent
 OUT = PKG / "libamg_b200.so"
 OBJDIR = HERE / "_build"
-SOURCES = ["amg_runtime.cu", "amg_drv_f64.cu", "amg_drv_f32.cu", "amg_drv_mixed.cu", "amg_capi.cu"]
+SOURCES = ["amg_runtime.cu", "amg_drv_f64.cu", "amg_drv_f32.cu", "amg_drv_mixed.cu", "amg_capi.cu",
+           "amg_noalloc.cu"]
 HEADERS = ["amg_device.cuh", "amg_runtime.cuh", str(ROOT / "include" / "amg_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

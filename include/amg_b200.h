@@ -140,6 +140,22 @@ amg_status amg_jacobi(const amg_csr* A, int32_t dtype, const void* x, const void
                       const void* dinv, void* out, int32_t k, int32_t iterations,
                       double omega, void* stream);
 
+/* amg_jacobi for callers that cannot allocate device memory when they call: a JAX/XLA
+ * custom call (XLA has already reserved most of the GPU and owns scratch allocation), an
+ * application on a fixed memory budget, a real-time caller that cannot afford an
+ * allocator call.  No counterpart in the reference (AMJax only runs inside JAX).
+ * Same arguments and results as amg_jacobi, but the iterate between sweeps lives in a
+ * 16 MiB device array compiled into this library (held on every GPU that loads the
+ * library until exit) instead of cudaMallocAsync; no cudaMalloc/cudaFree is called.
+ * Limit: with iterations >= 2, n_rows * k * element size must be <= 16 MiB, else
+ * AMG_ERR_INVALID_ARG.  The first call on a device looks up the array's device address
+ * (once per device, on the current device): make that first call before any stream
+ * capture.  All calls share the one array: calls whose work overlaps on the GPU (other
+ * streams, other threads) race on it. */
+amg_status amg_jacobi_noalloc(const amg_csr* A, int32_t dtype, const void* x, const void* b,
+                              const void* dinv, void* out, int32_t k, int32_t iterations,
+                              double omega, void* stream);
+
 /* y = A x for [n_cols, k] x (the BCOO ``A @ x`` of the reference, multilevel.py:321,335). */
 amg_status amg_spmv(const amg_csr* A, int32_t dtype, const void* x, void* y, int32_t k,
                     void* stream);
