@@ -21,6 +21,7 @@ void solve_plain(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     cy.fine_mask = q.k > 1; cy.red = red_of(pl);
     cy.visit(0, false, ct, q.cpl);
   };
+  autotune_cycle<T>(h, pl, q.k, A0, user);
   run_loop(pl, req_key("solve", q), user, prologue, body, [](cudaStream_t) {}, true, q.maxiter + 2);
 }
 
@@ -65,6 +66,18 @@ void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     OpCgDir<TO, TC> dir{p, z, pl->beta(), q.k, pl->stop()};
     run_elem<TC>(n0, dir, q.k, red_of(pl), cs, {p, z});
   };
+  autotune_cycle<TC>(h, pl, q.k, nullptr, user);
+  if (q.k > 1) {  // the outer CG ops, on scratch (the prologue resets every state they touch)
+    std::vector<int> ones(size_t(q.k), 1);
+    CK(cudaMemcpy(pl->active(), ones.data(), sizeof(int) * q.k, cudaMemcpyHostToDevice));
+    OpCgQ<TO> tq{p, nullptr, q.k, nullptr, pl->gamma(), pl->alpha()};
+    tune_op(*A0, tq, q.k, red_of(pl), user, {p});
+    OpCgUpdA<TO, TC> tu{};
+    tu.x = x; tu.r = r; tu.p = p; tu.r_lo = mixed ? rc : nullptr;
+    tu.alpha = pl->alpha(); tu.active = pl->active(); tu.ld = q.k; tu.stop = nullptr;
+    tu.ctl = make_ctl(pl, q.maxiter);
+    tune_op(*A0, tu, q.k, red_of(pl), user, {x, r, p, tu.r_lo});
+  }
   run_loop(pl, req_key("pcg", q), user, prologue, body, [](cudaStream_t) {}, true, q.maxiter + 2);
 }
 
@@ -77,6 +90,7 @@ void precondition(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     cy.b0 = static_cast<const T*>(q.b); cy.x0 = static_cast<T*>(q.x); cy.red = red_of(pl);
     cy.visit(0, true, ct, q.cpl);
   };
+  autotune_cycle<T>(h, pl, q.k, nullptr, user);
   run_loop(pl, req_key("prec", q), user, prologue, [](cudaStream_t) {}, [](cudaStream_t) {}, false, 0);
 }
 

@@ -33,6 +33,14 @@ void solve_mixed(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     OpRefine<double, float> up{x, e32, pl->active(), q.k, pl->stop()};
     run_elem<float>(n0, up, q.k, red_of(pl), cs, {x, e32});
   };
+  autotune_cycle<float>(h, pl, q.k, q.A0, user);
+  if (q.k > 1) {  // the outer residual, on scratch (its state is reset by the prologue)
+    OpResid<double, double, XS_PLAIN, false, float, true> tr{};
+    tr.xs = XSource<double, XS_PLAIN>{static_cast<const double*>(pl->p_out), b, nullptr, 1.0, q.k};
+    tr.b = b; tr.out = nullptr; tr.out_lo = r32; tr.ld = q.k; tr.stop = nullptr;
+    tr.ctl = make_ctl(pl, q.maxiter);
+    tune_op(*A0, tr, q.k, red_of(pl), user, {pl->p_out, b, r32});
+  }
   run_loop(pl, req_key("solve", q), user, prologue, body, [](cudaStream_t) {}, true, q.maxiter + 2);
 }
 
@@ -77,6 +85,18 @@ void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     OpCgDir<TO, TC> dir{p, z, pl->beta(), q.k, pl->stop()};
     run_elem<TC>(n0, dir, q.k, red_of(pl), cs, {p, z});
   };
+  autotune_cycle<TC>(h, pl, q.k, nullptr, user);
+  if (q.k > 1) {  // the outer CG ops, on scratch (the prologue resets every state they touch)
+    std::vector<int> ones(size_t(q.k), 1);
+    CK(cudaMemcpy(pl->active(), ones.data(), sizeof(int) * q.k, cudaMemcpyHostToDevice));
+    OpCgQ<TO> tq{p, nullptr, q.k, nullptr, pl->gamma(), pl->alpha()};
+    tune_op(*A0, tq, q.k, red_of(pl), user, {p});
+    OpCgUpdA<TO, TC> tu{};
+    tu.x = x; tu.r = r; tu.p = p; tu.r_lo = mixed ? rc : nullptr;
+    tu.alpha = pl->alpha(); tu.active = pl->active(); tu.ld = q.k; tu.stop = nullptr;
+    tu.ctl = make_ctl(pl, q.maxiter);
+    tune_op(*A0, tu, q.k, red_of(pl), user, {x, r, p, tu.r_lo});
+  }
   run_loop(pl, req_key("pcg", q), user, prologue, body, [](cudaStream_t) {}, true, q.maxiter + 2);
 }
 

@@ -1,5 +1,7 @@
 // amg_runtime.cu -- non-template host runtime: errors, device facts, plans, graph
 // construction (conditional WHILE node) and execution.
+#include <tuple>
+
 #include "amg_runtime.cuh"
 
 namespace amg {
@@ -33,6 +35,30 @@ DevInfo dev_info() {
 bool pdl_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("AMG_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<const void*, int64_t, int, int, int, const void*>, int> g_tune;
+}  // namespace
+
+int tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(std::make_tuple(rowptr, nnz, k, es, kv, tag));
+  return it == g_tune.end() ? 0 : it->second;
+}
+
+void set_tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag, int g) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[std::make_tuple(rowptr, nnz, k, es, kv, tag)] = g;
+}
+
+bool tuning_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("AMG_TUNE");
     return !(e && e[0] == '0');
   }();
   return on;

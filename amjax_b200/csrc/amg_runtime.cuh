@@ -236,8 +236,19 @@ static int pick_kv(int k, std::initializer_list<const void*> ptrs) {
   return kv;
 }
 
+// Autotuned lanes-per-row for a (matrix, k, value size, vector width, op type): 0 when
+// untuned.  op_tag<Op>() is a process-wide unique address per op type.
+int tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag);
+
+template <class Op>
+const void* op_tag() {
+  static const char tag = 0;
+  return &tag;
+}
+
 template <class T>
-static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> ptrs) {
+static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> ptrs,
+                 const void* tune_rowptr = nullptr, int64_t tune_nnz = 0, const void* tune_tag = nullptr) {
   Cfg c;
   const DevInfo d = dev_info();
   if (k == 1) {
@@ -247,10 +258,19 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     c.KV = pick_kv<T>(k, ptrs);
     const int nch = k / c.KV;
     c.G = std::max(4, std::min(32, pow2ceil(nch)));
+    if (tune_rowptr) {
+      const int tg = tuned_g(tune_rowptr, tune_nnz, k, int(sizeof(T)), c.KV, tune_tag);
+      if (tg) c.G = tg;
+    }
+    if (const char* fg = std::getenv("AMG_KB_G")) {  // manual override (experiments)
+      const int g = atoi(fg);
+      if (g == 4 || g == 8 || g == 16 || g == 32) c.G = g;
+    }
     const int per = (nch + c.G - 1) / c.G;
     if (per > kMaxCh)
       fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);
     c.NCH = per <= 1 ? 1 : per <= 2 ? 2 : 4;
+    if (c.KV == 1 && c.NCH > 1) c.G = 32;
     c.smem = sizeof(double) * std::max<size_t>(size_t(kBlock / c.G) * k, kBlock);
   }
   const int rows_per_cta = kBlock / c.G;
@@ -309,17 +329,28 @@ static void launch_kb(const Csr& M, const typename Op::V* vals, const Op& op, co
   launch(csr_kb<Op, G, KV, NCH>, grid, kBlock, c.smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
 }
 
-// (G, NCH) pairs: NCH = 1 for any G; NCH > 1 only with G = 32.
+// (G, NCH) pairs: any G in {4, 8, 16, 32} with NCH in {1, 2, 4} for vector widths >= 2;
+// scalar columns (odd k) use NCH = 1, or G = 32 with NCH in {2, 4}.
+template <class Op, int KV, int G>
+static void dispatch_kb_nch(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
+                            RedCtx rc, cudaStream_t s) {
+  if (c.NCH == 1) launch_kb<Op, G, KV, 1>(M, vals, op, c, rc, s);
+  else if constexpr (KV >= 2 || G == 32) {
+    if (c.NCH == 2) launch_kb<Op, G, KV, 2>(M, vals, op, c, rc, s);
+    else launch_kb<Op, G, KV, 4>(M, vals, op, c, rc, s);
+  } else {
+    fail(AMG_ERR_INVALID_ARG, "internal: (G=%d, NCH=%d) not built for scalar columns", G, c.NCH);
+  }
+}
+
 template <class Op, int KV>
 static void dispatch_kb_g(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                           RedCtx rc, cudaStream_t s) {
-  if (c.NCH == 2) { launch_kb<Op, 32, KV, 2>(M, vals, op, c, rc, s); return; }
-  if (c.NCH == 4) { launch_kb<Op, 32, KV, 4>(M, vals, op, c, rc, s); return; }
   switch (c.G) {
-    case 4: launch_kb<Op, 4, KV, 1>(M, vals, op, c, rc, s); break;
-    case 8: launch_kb<Op, 8, KV, 1>(M, vals, op, c, rc, s); break;
-    case 16: launch_kb<Op, 16, KV, 1>(M, vals, op, c, rc, s); break;
-    default: launch_kb<Op, 32, KV, 1>(M, vals, op, c, rc, s); break;
+    case 4: dispatch_kb_nch<Op, KV, 4>(M, vals, op, c, rc, s); break;
+    case 8: dispatch_kb_nch<Op, KV, 8>(M, vals, op, c, rc, s); break;
+    case 16: dispatch_kb_nch<Op, KV, 16>(M, vals, op, c, rc, s); break;
+    default: dispatch_kb_nch<Op, KV, 32>(M, vals, op, c, rc, s); break;
   }
 }
 
@@ -330,7 +361,7 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
   using V = typename Op::V;
   const V* vals = M.template vals<V>();
   if (M.nnz > 0 && !vals) fail(AMG_ERR_INVALID_ARG, "matrix values missing for this precision");
-  const Cfg c = cfg_k<typename Op::Acc>(M.n_rows, k, M.g1, ptrs);
+  const Cfg c = cfg_k<typename Op::Acc>(M.n_rows, k, M.g1, ptrs, M.rowptr, M.nnz, op_tag<Op>());
   RedCtx rc{red.partials, red.counter, k};
   if (op.reduces() && !red.partials) fail(AMG_ERR_INVALID_ARG, "reduction scratch missing");
   if (k == 1) {
@@ -349,6 +380,126 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
     else fail(AMG_ERR_INVALID_ARG, "internal: 4-wide FP64 vectors");
   }
   CK_LAUNCH();
+}
+
+// ------------------------------------------------------------------ autotuner
+// Record the fastest lanes-per-row for (matrix, k, value size, vector width, op type).
+void set_tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag, int g);
+bool tuning_enabled();
+
+// Time one fused CSR op (a fully formed instance on scratch buffers, stop flag off) with
+// each candidate lanes-per-row G (each with its chunks per lane) and keep the fastest for
+// this (matrix, k, type, op).  Runs outside stream capture, once per key.
+template <class Op>
+void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
+             std::initializer_list<const void*> ptrs) {
+  using T = typename Op::Acc;
+  if (k == 1 || M.n_rows == 0) return;
+  if (M.nnz > 0 && !M.template vals<typename Op::V>()) return;
+  const int kv = pick_kv<T>(k, ptrs);
+  if (!tuning_enabled()) return;
+  const void* tag = op_tag<Op>();
+  if (tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag)) return;
+  const int nch = k / kv;
+  const int gmax = std::max(4, std::min(32, pow2ceil(nch)));
+  std::vector<int> cands;
+  for (int g = 4; g <= gmax; g <<= 1) {
+    const int per = (nch + g - 1) / g;
+    if (per <= kMaxCh && (kv > 1 || per == 1 || g == 32)) cands.push_back(g);
+  }
+  if (cands.size() <= 1) {
+    set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, cands.empty() ? gmax : cands[0]);
+    return;
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int best = cands.back();
+  float best_t = 1e30f;
+  for (int g : cands) {
+    set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, g);
+    run_csr(M, op, k, red, s, ptrs);
+    float tmin = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      CK(cudaEventRecord(e0, s));
+      run_csr(M, op, k, red, s, ptrs);
+      CK(cudaEventRecord(e1, s));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      tmin = std::min(tmin, ms);
+    }
+    if (tmin < best_t) {
+      best_t = tmin;
+      best = g;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, best);
+  if (std::getenv("AMG_TUNE_LOG"))
+    fprintf(stderr, "[amg tune] rows=%d nnz=%lld k=%d es=%d kv=%d op=%p -> G=%d (%.1f us)\\n", M.n_rows,
+            (long long)M.nnz, k, int(sizeof(T)), kv, tag, best, best_t * 1e3f);
+}
+
+// Tune the cycle's ops in type T on every level (Jacobi sweeps, residuals, restriction,
+// prolongation) for this plan's k; level 0 uses A0 when given.
+template <class T>
+void autotune_cycle(amg_hierarchy* h, Plan* pl, int k, const Csr* A0, cudaStream_t s) {
+  if (k == 1) return;
+  const int L = int(h->levels.size());
+  for (int l = 0; l < L - 1; ++l) {
+    const Level& lv = h->levels[l];
+    const Csr& A = (l == 0 && A0) ? *A0 : lv.A;
+    T* w1 = static_cast<T*>(pl->W1[l]);
+    T* w2 = static_cast<T*>(pl->W2[l]);
+    T* bl = static_cast<T*>(pl->B[l]);
+    T* xc = static_cast<T*>(pl->X[l + 1]);
+    T* bc = static_cast<T*>(pl->B[l + 1]);
+    const T* dv = lv.template dinv<T>();
+    if (!dv) continue;
+    {
+      OpJacobi<T, XS_PLAIN> op{};
+      op.xs = XSource<T, XS_PLAIN>{w1, bl, dv, T(0.5), k};
+      op.b = bl; op.dinv = dv; op.omega = T(0.5); op.out = w2; op.ld = k;
+      tune_op(A, op, k, Red{}, s, {w1, bl, w2});
+    }
+    {
+      OpJacobi<T, XS_JAC0> op{};
+      op.xs = XSource<T, XS_JAC0>{nullptr, bl, dv, T(0.5), k};
+      op.b = bl; op.dinv = dv; op.omega = T(0.5); op.out = w2; op.ld = k;
+      tune_op(A, op, k, Red{}, s, {bl, w2});
+    }
+    {
+      OpResid<T, T, XS_PLAIN, true, T, false> op{};
+      op.xs = XSource<T, XS_PLAIN>{w1, bl, dv, T(0.5), k};
+      op.b = bl; op.out = w2; op.ld = k;
+      tune_op(A, op, k, Red{}, s, {w1, bl, w2});
+    }
+    {
+      OpResid<T, T, XS_JAC0, true, T, false> op{};
+      op.xs = XSource<T, XS_JAC0>{nullptr, bl, dv, T(0.5), k};
+      op.b = bl; op.out = w2; op.ld = k;
+      tune_op(A, op, k, Red{}, s, {bl, w2});
+    }
+    {
+      OpAxpy<T, XS_ZERO> op{};
+      op.x = w2; op.out = bc; op.ld = k;
+      tune_op(lv.R, op, k, Red{}, s, {w2, bc});
+    }
+    {
+      OpAxpy<T, XS_PLAIN> op{};
+      op.base = XSource<T, XS_PLAIN>{w1, bl, dv, T(0), k};
+      op.x = xc; op.out = w2; op.ld = k;
+      tune_op(lv.P, op, k, Red{}, s, {w1, xc, w2});
+    }
+    {
+      OpAxpy<T, XS_JAC0> op{};
+      op.base = XSource<T, XS_JAC0>{nullptr, bl, dv, T(0.5), k};
+      op.x = xc; op.out = w1; op.ld = k;
+      tune_op(lv.P, op, k, Red{}, s, {bl, xc, w1});
+    }
+  }
 }
 
 template <class Op, int G, int KV, int NCH>
