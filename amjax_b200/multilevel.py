@@ -285,6 +285,9 @@ class MultilevelSolver:
     def _override(self, A):
         if A is None:
             return None
+        from .autograd import SparseA
+        if isinstance(A, SparseA):
+            A = A.csr()
         M = CSRMatrix.from_any(A, dtype=self.dtype, device=self.levels[0].A.device)
         if M.shape != self.levels[0].A.shape:
             raise ValueError(f"A has shape {M.shape}, expected {self.levels[0].A.shape}")
