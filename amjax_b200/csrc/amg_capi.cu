@@ -13,6 +13,16 @@ static void jacobi_impl(const amg_csr* Ad, const void* x, const void* b, const v
   if (iterations > 1) CK(cudaMallocAsync(reinterpret_cast<void**>(&tmp), bytes, s));
   try {
     const T* in = static_cast<const T*>(x);
+    if (k > 1) {  // pick the layout once per (matrix, k, type); tuning writes only `out`
+      OpJacobi<T, XS_PLAIN> top{};
+      top.xs = XSource<T, XS_PLAIN>{in, static_cast<const T*>(b), static_cast<const T*>(dinv), T(omega), k};
+      top.b = static_cast<const T*>(b);
+      top.dinv = static_cast<const T*>(dinv);
+      top.omega = T(omega);
+      top.out = static_cast<T*>(out);
+      top.ld = k;
+      tune_op(A, top, k, Red{}, s, {in, b, out});
+    }
     for (int i = 0; i < iterations; ++i) {
       T* o = ((iterations - 1 - i) % 2 == 0) ? static_cast<T*>(out) : tmp;
       OpJacobi<T, XS_PLAIN> op{};
@@ -197,10 +207,12 @@ amg_status amg_spmv(const amg_csr* A, int32_t dtype, const void* x, void* y, int
     if (dtype == 0) {
       OpAxpy<double, XS_ZERO> op{};
       op.x = static_cast<const double*>(x); op.out = static_cast<double*>(y); op.ld = k;
+      tune_op(M, op, k, Red{}, s, {x, y});
       run_csr(M, op, k, Red{}, s, {x, y});
     } else if (dtype == 1) {
       OpAxpy<float, XS_ZERO> op{};
       op.x = static_cast<const float*>(x); op.out = static_cast<float*>(y); op.ld = k;
+      tune_op(M, op, k, Red{}, s, {x, y});
       run_csr(M, op, k, Red{}, s, {x, y});
     } else {
       fail(AMG_ERR_INVALID_ARG, "dtype must be 0 (FP64) or 1 (FP32)");

@@ -438,7 +438,7 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
   cudaEventDestroy(e1);
   set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, best);
   if (std::getenv("AMG_TUNE_LOG"))
-    fprintf(stderr, "[amg tune] rows=%d nnz=%lld k=%d es=%d kv=%d op=%p -> G=%d (%.1f us)\\n", M.n_rows,
+    fprintf(stderr, "[amg tune] rows=%d nnz=%lld k=%d es=%d kv=%d op=%p -> G=%d (%.1f us)\n", M.n_rows,
             (long long)M.nnz, k, int(sizeof(T)), kv, tag, best, best_t * 1e3f);
 }
 
