@@ -12,6 +12,7 @@ from .relaxation.relaxation import jacobi, inverse_diagonal
 from .csr import CSRMatrix
 from .autograd import SparseA
 from .krylov import cg
+from .batch import pcg_batch
 
 __all__ = [
     "MultilevelSolver",
@@ -21,6 +22,7 @@ __all__ = [
     "CSRMatrix",
     "SparseA",
     "cg",
+    "pcg_batch",
     "multilevel_solver",
     "coarse_grid_solver",
 ]

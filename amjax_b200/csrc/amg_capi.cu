@@ -4,6 +4,35 @@
 // ======================================================================= C ABI
 using namespace amg;
 
+template <class TO, class TC>
+static void pcg_batch_impl(amg_hierarchy* const* hs, int nsys, int precision, const void* const* b,
+                           void* const* x, const int32_t* k, double tol, double atol, int maxiter,
+                           int cycle, int cpl, int32_t* iters_out, double* relres_out, cudaStream_t s) {
+  std::vector<BatchSys> sys;
+  std::vector<Plan*> plans;
+  std::string key = "batch";
+  for (int i = 0; i < nsys; ++i) {
+    Plan* pl = get_plan(hs[i], precision, k[i], s);
+    Req q{precision, k[i], cycle, cpl, maxiter, tol, atol, b[i], x[i], nullptr};
+    BatchSys bs;
+    bs.pl = pl;
+    bs.gmax = maxiter + 2;
+    pcg_emit<TO, TC>(hs[i], pl, q, s, &bs.pro, &bs.body);
+    sys.push_back(std::move(bs));
+    plans.push_back(pl);
+    char buf[48];
+    snprintf(buf, sizeof(buf), "/%p:", (void*)hs[i]);
+    key += buf + req_key("pcg", q);
+  }
+  run_batch(sys, key, s);
+  size_t off = 0;
+  for (int i = 0; i < nsys; ++i) {
+    read_results(plans[size_t(i)], s, true, iters_out ? iters_out + off : nullptr,
+                 relres_out ? relres_out + off : nullptr);
+    off += size_t(k[i]);
+  }
+}
+
 template <class T>
 static void jacobi_impl(const amg_csr* Ad, const void* x, const void* b, const void* dinv, void* out,
                         int k, int iterations, double omega, cudaStream_t s) {
@@ -245,6 +274,39 @@ amg_status amg_sampled_outer(const amg_csr* A, const double* lam, const double* 
     const int grid = std::max(1, std::min((A->n_rows + 7) / 8, dev_info().max_ctas));
     sampled_outer_kernel<<<grid, 256, 0, s>>>(A->rowptr, A->col, A->n_rows, lam, x, k, grad);
     CK_LAUNCH();
+  });
+}
+
+amg_status amg_pcg_batch(amg_hierarchy* const* hs, int32_t nsys, int32_t precision,
+                         const void* const* b, void* const* x, const int32_t* k, double tol,
+                         double atol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
+                         int32_t* iters_out, double* relres_out, void* stream) {
+  return guarded([&] {
+    if (nsys < 1 || !hs || !b || !x || !k) fail(AMG_ERR_INVALID_ARG, "empty or null batch");
+    if (maxiter < 0) fail(AMG_ERR_INVALID_ARG, "maxiter must be >= 0");
+    cycle_char(cycle);
+    std::vector<amg_hierarchy*> uniq(hs, hs + nsys);
+    for (int i = 0; i < nsys; ++i) {
+      if (!hs[i]) fail(AMG_ERR_INVALID_ARG, "system %d: null hierarchy", i);
+      check_vec(b[i], "b");
+      check_vec(x[i], "x");
+      if (k[i] < 1) fail(AMG_ERR_INVALID_ARG, "system %d: k must be >= 1", i);
+    }
+    std::sort(uniq.begin(), uniq.end());
+    if (std::adjacent_find(uniq.begin(), uniq.end()) != uniq.end())
+      fail(AMG_ERR_INVALID_ARG, "a hierarchy appears twice in one batch");
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (amg_hierarchy* hh : uniq) locks.emplace_back(hh->mu);  // address order: no deadlock
+    for (int i = 0; i < nsys; ++i) check_prec_data(hs[i], precision, nullptr);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == AMG_PREC_F64)
+      pcg_batch_impl<double, double>(hs, nsys, precision, b, x, k, tol, atol, maxiter, cycle, cycles_per_level, iters_out, relres_out, s);
+    else if (precision == AMG_PREC_F32)
+      pcg_batch_impl<float, float>(hs, nsys, precision, b, x, k, tol, atol, maxiter, cycle, cycles_per_level, iters_out, relres_out, s);
+    else if (precision == AMG_PREC_MIXED)
+      pcg_batch_impl<double, float>(hs, nsys, precision, b, x, k, tol, atol, maxiter, cycle, cycles_per_level, iters_out, relres_out, s);
+    else
+      fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
   });
 }
 

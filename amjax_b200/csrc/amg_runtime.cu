@@ -311,6 +311,70 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
   }
 }
 
+namespace {
+std::mutex g_batch_mu;
+std::list<std::pair<std::string, std::unique_ptr<GraphEntry>>> g_batch_graphs;  // LRU of 4
+}  // namespace
+
+void run_batch(const std::vector<BatchSys>& systems, const std::string& key, cudaStream_t user) {
+  std::lock_guard<std::mutex> lk(g_batch_mu);
+  GraphEntry* ge = nullptr;
+  for (auto it = g_batch_graphs.begin(); it != g_batch_graphs.end(); ++it) {
+    if (it->first == key) {
+      g_batch_graphs.splice(g_batch_graphs.begin(), g_batch_graphs, it);
+      ge = g_batch_graphs.front().second.get();
+      break;
+    }
+  }
+  if (!ge) {
+    auto e = std::make_unique<GraphEntry>();
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    e->graph = g;
+    cudaStream_t cs = capture_stream();
+    for (const BatchSys& sy : systems) {
+      // prologue as a new root branch; its last nodes come from the capture state
+      CK(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      std::vector<cudaGraphNode_t> dep;
+      try {
+        sy.pro(cs);
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* d = nullptr;
+        size_t nd = 0;
+        CK(cudaStreamGetCaptureInfo(cs, &st, nullptr, nullptr, &d, &nd));
+        dep.assign(d, d + nd);
+      } catch (...) {
+        cudaGraph_t junk = g;
+        cudaStreamEndCapture(cs, &junk);
+        throw;
+      }
+      cudaGraph_t g2 = g;
+      CK(cudaStreamEndCapture(cs, &g2));
+      cudaGraphConditionalHandle hc;
+      CK(cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+      cp.conditional.handle = hc;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cn;
+      CK(cudaGraphAddNode(&cn, g, dep.empty() ? nullptr : dep.data(), dep.size(), &cp));
+      cudaGraph_t bg = cp.conditional.phGraph_out[0];
+      int* stp = sy.pl->stop();
+      int* gc = sy.pl->gcount();
+      const int gmax = sy.gmax;
+      capture(bg, nullptr, 0, [&](cudaStream_t c2) {
+        sy.body(c2);
+        launch(loop_guard_kernel, 1, 32, 0, c2, stp, gc, gmax, hc);
+      });
+    }
+    CK(cudaGraphInstantiate(&e->exec, g, 0));
+    g_batch_graphs.emplace_front(key, std::move(e));
+    while (g_batch_graphs.size() > 4) g_batch_graphs.pop_back();
+    ge = g_batch_graphs.front().second.get();
+  }
+  CK(cudaGraphLaunch(ge->exec, user));
+}
+
 void read_results(Plan* pl, cudaStream_t s, bool cg, int32_t* iters_out, double* relres_out) {
   if (!iters_out && !relres_out) return;
   const int k = pl->k;

@@ -841,6 +841,18 @@ inline void emit_setup(Plan* pl, cudaStream_t cs, int n0, const T* b, T* dst, TL
 template <class T> void solve_plain(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 void solve_mixed(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 template <class TO, class TC> void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
+template <class TO, class TC>
+void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit* pro, Emit* bod);
+
+// One system of a batch: its plan and its emitters (prologue, loop body).
+struct BatchSys {
+  Plan* pl;
+  Emit pro, body;
+  int gmax;
+};
+// Capture (once per key) and launch one graph holding every system's loop as an independent
+// branch (its own conditional WHILE node), so one launch solves them all concurrently.
+void run_batch(const std::vector<BatchSys>& systems, const std::string& key, cudaStream_t user);
 template <class T> void precondition(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 
 // per-translation-unit kernel counters (each TU owns a copy of g_kernel_count)

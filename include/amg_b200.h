@@ -134,6 +134,17 @@ amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, 
                    int32_t cycles_per_level, const amg_csr* A0, int32_t* iters_out,
                    double* relres_out, void* stream);
 
+/* Several independent PCG solves in one graph launch: system i uses hierarchy hs[i], its own
+ * k[i] right-hand sides b[i] -> x[i] (layouts as in amg_pcg), and the shared tol / atol /
+ * maxiter / cycle.  The reference solves one system per call (jax.vmap batches right-hand
+ * sides of one hierarchy only, README.md:60-66); this runs many hierarchies of different
+ * sizes concurrently, each with its own convergence loop.  iters_out / relres_out (nullable)
+ * get sum(k) entries, system after system.  Each hierarchy may appear once per call. */
+amg_status amg_pcg_batch(amg_hierarchy* const* hs, int32_t nsys, int32_t precision,
+                         const void* const* b, void* const* x, const int32_t* k, double tol,
+                         double atol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
+                         int32_t* iters_out, double* relres_out, void* stream);
+
 /* Damped Jacobi sweeps on one CSR matrix (amjax/relaxation/relaxation.py:64-98).
  * dtype 0 = FP64 (x, b, dinv, out double), 1 = FP32.  out may not alias x. */
 amg_status amg_jacobi(const amg_csr* A, int32_t dtype, const void* x, const void* b,
