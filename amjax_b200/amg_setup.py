@@ -76,30 +76,43 @@ def _csr(A):
     return A
 
 
-def _rho_dinv_a(A):
-    """Largest |eigenvalue| of D^-1 A (ARPACK, with a power-iteration fallback)."""
+def _rho_dinv_a(A, steps=15):
+    """Estimate of rho(D^-1 A) for the prolongator-smoothing weight.
+
+    Symmetric A: ``steps`` Arnoldi (= Lanczos) steps on D^-1 A from a seeded random start,
+    rho = the largest Ritz value (the short Krylov estimate the smoothed-aggregation
+    literature uses; for a symmetric-similar operator Ritz values lie inside the spectrum).
+    Nonsymmetric A: ARPACK, since Ritz values of a non-normal operator can overshoot.
+    Exact eigenvalues for small matrices."""
     d = A.diagonal()
     dinv = np.where(d != 0, 1.0 / np.where(d != 0, d, 1.0), 0.0)
-    DA = sp.diags(dinv) @ A
     n = A.shape[0]
     if n <= 64:
-        ev = np.linalg.eigvals(DA.toarray())
-        return float(np.max(np.abs(ev)))
-    try:
-        v0 = np.random.default_rng(0).standard_normal(n)
-        ev = spla.eigs(DA, k=1, which="LM", return_eigenvectors=False, v0=v0, tol=1e-4, maxiter=200)
-        return float(np.abs(ev[0]))
-    except Exception:  # ARPACK did not converge: fall back to power iteration
-        v = np.random.default_rng(0).standard_normal(n)
-        v /= np.linalg.norm(v)
-        rho = 1.0
-        for _ in range(50):
-            w = DA @ v
-            rho = np.linalg.norm(w)
-            if rho == 0:
-                break
-            v = w / rho
-        return float(rho)
+        return float(np.max(np.abs(np.linalg.eigvals((sp.diags(dinv) @ A).toarray()))))
+    if (A != A.T).nnz != 0:
+        DA = sp.diags(dinv) @ A
+        try:
+            v0 = np.random.default_rng(0).standard_normal(n)
+            ev = spla.eigs(DA, k=1, which="LM", return_eigenvectors=False, v0=v0, tol=1e-4, maxiter=400)
+            return float(np.abs(ev[0]))
+        except Exception:
+            pass
+    m = min(steps, n)
+    V = np.zeros((m + 1, n))
+    H = np.zeros((m + 1, m))
+    v = np.random.default_rng(0).standard_normal(n)
+    V[0] = v / np.linalg.norm(v)
+    for j in range(m):
+        w = dinv * (A @ V[j])
+        for i in range(j + 1):
+            H[i, j] = w @ V[i]
+            w = w - H[i, j] * V[i]
+        H[j + 1, j] = np.linalg.norm(w)
+        if H[j + 1, j] < 1e-14:
+            m = j + 1
+            break
+        V[j + 1] = w / H[j + 1, j]
+    return float(np.max(np.abs(np.linalg.eigvals(H[:m, :m]))))
 
 
 # ---------------------------------------------------------------- smoothed aggregation

@@ -57,6 +57,12 @@ def parse():
                    help="only launch the dominant kernel (fine-level FP32 Jacobi sweep, k columns) a few "
                         "times: the command the ncu captures of that kernel run")
     p.add_argument("--kernel-reps", type=int, default=3)
+    p.add_argument("--ragged", action="store_true",
+                   help="config 3b: 24 SA hierarchies (2D, n ~ U{64..1024} from default_rng(1), odd i "
+                        "rotated anisotropic), k_i ~ U{1..16}, mixed PCG to 1e-8 in one graph launch")
+    p.add_argument("--cube", action="store_true",
+                   help="config 4: 3D 7-point lognormal-kappa diffusion 128^3, V/W/F, k = 1 and 16, "
+                        "FP32-cycle refinement to 1e-10 vs FP64; error vs a direct solve at 48^3")
     p.add_argument("--kernel", default="jacobi32", choices=["jacobi32", "pcg"],
                    help="--kernel-only target: the FP32 Jacobi sweep alone, or --kernel-reps CG steps of "
                         "the headline solve (every kernel of the CG loop)")
@@ -442,8 +448,103 @@ def run_kernel_only(args):
     return 0
 
 
+def _time_ms(fn, steps, warmup):
+    import torch
+    ts = timed_steps(fn, steps, warmup, lambda: None)
+    return statistics.mean(ts), min(ts)
+
+
+def run_ragged(args):
+    """Config 3b.  Draw order: for i in 0..23, n_i then k_i from default_rng(1); system i's
+    right-hand sides from default_rng(100 + i).  Even i: 5-point Poisson n_i^2; odd i: rotated
+    (45 degree) anisotropic diffusion with epsilon 1e-2 (i = 1, 5, 9, ...) or 1e-3."""
+    import torch
+    from amjax_b200 import MultilevelSolver, amg_setup, gallery, pcg_batch
+    rng = np.random.default_rng(1)
+    draws = [(int(rng.integers(64, 1025)), int(rng.integers(1, 17))) for _ in range(24)]
+    spec = ("jacobi", {"iterations": 1, "omega": 2.0 / 3.0})
+    mls, rhs, mats = [], [], []
+    t0 = time.perf_counter()
+    for i, (n, k) in enumerate(draws):
+        A = gallery.poisson((n, n)) if i % 2 == 0 else gallery.anisotropic_diffusion_2d(
+            n, 1e-2 if (i // 2) % 2 == 0 else 1e-3, np.pi / 4)
+        mls.append(MultilevelSolver.from_pyamg(amg_setup.smoothed_aggregation_solver(A),
+                                               presmoother=spec, postsmoother=spec))
+        rhs.append(torch.as_tensor(np.random.default_rng(100 + i).standard_normal((A.shape[0], k))).cuda())
+        mats.append(A)
+    setup_s = time.perf_counter() - t0
+    batch = lambda: pcg_batch(mls, rhs, tol=1e-8, maxiter=500, precision="mixed")
+    seq = lambda: [m.pcg(b, tol=1e-8, maxiter=500, precision="mixed") for m, b in zip(mls, rhs)]
+    tb, tbmin = _time_ms(batch, args.steps, args.warmup)
+    tsq, tsqmin = _time_ms(seq, args.steps, args.warmup)
+    X, info = pcg_batch(mls, rhs, tol=1e-8, maxiter=500, precision="mixed", return_info=True)
+    rel = []
+    for A, b, x in zip(mats, rhs, X):
+        bn, xn = b.cpu().numpy(), x.cpu().numpy()
+        rel.append(float((np.linalg.norm(bn - A @ xn, axis=0) / np.linalg.norm(bn, axis=0)).max()))
+    line = {"mode": "ragged", "metric": "ms per batch of 24 hierarchies (mixed PCG to 1e-8)",
+            "value": tb, "unit": "ms/batch", "ms_min": tbmin, "sequential_ms": tsq,
+            "speedup_vs_sequential": tsq / tb, "systems": 24,
+            "rows": [A.shape[0] for A in mats], "rhs": [k for _, k in draws],
+            "total_rows": int(sum(A.shape[0] for A in mats)), "total_rhs": int(sum(k for _, k in draws)),
+            "iterations_max": [max(d["iterations"]) for d in info], "relres_fp64_max": max(rel),
+            "host_setup_s": setup_s, "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_cube(args):
+    """Config 4: -div(kappa grad u) on 128^3 cells (N = 2,097,152), kappa = exp(g), g ~ N(0,1)
+    from default_rng(2), harmonic face means, Dirichlet; SA; Jacobi 2/3; pinv.  Standalone
+    solves to 1e-10: FP64 cycle vs FP32 cycle inside FP64 refinement, V / W / F, k = 1 and
+    16.  True error against a direct solve on the 48^3 subsize."""
+    import torch
+    import scipy.sparse.linalg as spla
+    from amjax_b200 import MultilevelSolver, amg_setup, gallery
+    spec = ("jacobi", {"iterations": 1, "omega": 2.0 / 3.0})
+    out = {"mode": "cube", "data": "synthetic", "tol": 1e-10}
+    t0 = time.perf_counter()
+    A = gallery.variable_diffusion_3d(128, sigma=1.0, seed=2)
+    ml = MultilevelSolver.from_pyamg(amg_setup.smoothed_aggregation_solver(A), presmoother=spec, postsmoother=spec)
+    out["host_setup_s"] = time.perf_counter() - t0
+    out["levels"] = [l.A.shape[0] for l in ml.levels]
+    res = {}
+    for k in (1, 16):
+        Bh = np.random.default_rng(2).standard_normal((A.shape[0], k) if k > 1 else A.shape[0])
+        B = torch.as_tensor(Bh).cuda()
+        for cyc in "VWF":
+            for prec in ("f64", "mixed"):
+                p = ml._precision(prec)
+                f = lambda: ml._solve_dev(B, None, 1e-10, 300, cyc, 1, p)
+                ms, msmin = _time_ms(f, max(2, args.steps // 3), 1)
+                x, info = f()
+                xn = x.cpu().numpy()
+                r = np.linalg.norm((Bh - A @ xn).reshape(A.shape[0], -1), axis=0) / \
+                    np.linalg.norm(Bh.reshape(A.shape[0], -1), axis=0)
+                res[f"k{k}_{cyc}_{prec}"] = {"ms": ms, "iterations": max(info["iterations"]),
+                                             "relres_fp64_max": float(r.max())}
+    for k in (1, 16):
+        for cyc in "VWF":
+            a, b = res[f"k{k}_{cyc}_f64"]["ms"], res[f"k{k}_{cyc}_mixed"]["ms"]
+            res[f"k{k}_{cyc}_speedup_mixed"] = a / b
+    out["solves"] = res
+    As = gallery.variable_diffusion_3d(48, sigma=1.0, seed=2)
+    ms_ = MultilevelSolver.from_pyamg(amg_setup.smoothed_aggregation_solver(As), presmoother=spec, postsmoother=spec)
+    bs = np.random.default_rng(2).standard_normal(As.shape[0])
+    xd = spla.splu(As.tocsc()).solve(bs)
+    for prec in ("f64", "mixed"):
+        xs = ms_.solve(bs, tol=1e-10, maxiter=300, precision=prec)
+        out[f"err_vs_direct_48cube_{prec}"] = float(np.linalg.norm(xs - xd) / np.linalg.norm(xd))
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.ragged:
+        return run_ragged(args)
+    if args.cube:
+        return run_cube(args)
     if args.kernel_only:
         return run_kernel_only(args)
     if args.impl == "reference":
