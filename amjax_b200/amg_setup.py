@@ -40,6 +40,7 @@ __all__ = [
     "HostHierarchy",
     "smoothed_aggregation_solver",
     "ruge_stuben_solver",
+    "air_solver",
     "save_hierarchy",
     "load_hierarchy",
 ]
@@ -324,6 +325,81 @@ def ruge_stuben_solver(A, max_levels=10, max_coarse=10, theta=0.25, **_ignored):
         levels[-1].R = R
         levels.append(HostLevel(_csr(R @ A @ P)))
     return HostHierarchy(levels, kind="ruge_stuben")
+
+
+# ---------------------------------------------------------------- AIR (nonsymmetric)
+
+def _one_point_interpolation(A, S, is_c):
+    """Each C point injects itself; each F point takes the value of its strongest C
+    neighbour (largest |a_ij| among strong C connections), weight 1; F points without one
+    get a zero row."""
+    n = A.shape[0]
+    cidx = np.cumsum(is_c) - 1
+    Sc = S.tocoo()
+    A_abs = abs(A).tocsr()
+    vals = np.asarray(A_abs[Sc.row, Sc.col]).ravel()
+    keep = is_c[Sc.col] & ~is_c[Sc.row]
+    r, c, v = Sc.row[keep], Sc.col[keep], vals[keep]
+    best = np.full(n, -1)
+    bestv = np.full(n, -np.inf)
+    order = np.lexsort((c, -v))  # strongest first, ties by column
+    for ri, ci, vi in zip(r[order], c[order], v[order]):
+        if best[ri] < 0:
+            best[ri] = ci
+            bestv[ri] = vi
+    crow = np.nonzero(is_c)[0]
+    frow = np.nonzero((~is_c) & (best >= 0))[0]
+    rows = np.concatenate([crow, frow])
+    cols = np.concatenate([cidx[crow], cidx[best[frow]]])
+    return _csr(sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(n, int(is_c.sum()))))
+
+
+def _air_restriction(A, S, is_c):
+    """Distance-1 approximate ideal restriction.  The ideal restriction is
+    R = [-A_cf A_ff^-1, I]; row i of R (a C point) is approximated on the F points N_i it
+    strongly depends on by solving the local system z^T A[N_i, N_i] = -A[i, N_i], and
+    carries 1 at i itself."""
+    n = A.shape[0]
+    cidx = np.cumsum(is_c) - 1
+    A = _csr(A)
+    S = _csr(S)
+    rows, cols, vals = [], [], []
+    for i in np.nonzero(is_c)[0]:
+        nb = S.indices[S.indptr[i]:S.indptr[i + 1]]
+        Ni = nb[~is_c[nb]]
+        rows.append(cidx[i]); cols.append(i); vals.append(1.0)
+        if len(Ni) == 0:
+            continue
+        Aff = A[Ni][:, Ni].toarray()
+        aif = A[i, Ni].toarray().ravel()
+        try:
+            z = np.linalg.solve(Aff.T, -aif)
+        except np.linalg.LinAlgError:
+            z = np.linalg.lstsq(Aff.T, -aif, rcond=None)[0]
+        rows.extend([cidx[i]] * len(Ni)); cols.extend(Ni.tolist()); vals.extend(z.tolist())
+    return _csr(sp.csr_matrix((vals, (rows, cols)), shape=(int(is_c.sum()), n)))
+
+
+def air_solver(A, max_levels=10, max_coarse=20, theta=0.3, **_ignored):
+    """Approximate-ideal-restriction AMG for nonsymmetric (advection-dominated) problems
+    (Manteuffel, Ruge, Southworth, SISC 2018): classical strength (theta = 0.3 on |a_ij|),
+    first-pass Ruge-Stueben C/F splitting, one-point interpolation, distance-1 AIR
+    restriction, Galerkin coarse operators R A P; R is not P^T."""
+    A = _csr(A).astype(np.float64)
+    levels = [HostLevel(A)]
+    while len(levels) < max_levels and levels[-1].A.shape[0] > max_coarse:
+        A = levels[-1].A
+        S = _classical_strength(A, theta)
+        is_c = _rs_first_pass(S)
+        nc = int(is_c.sum())
+        if nc == 0 or nc >= A.shape[0]:
+            break
+        P = _one_point_interpolation(A, S, is_c)
+        R = _air_restriction(A, S, is_c)
+        levels[-1].P = P
+        levels[-1].R = R
+        levels.append(HostLevel(_csr(R @ A @ P)))
+    return HostHierarchy(levels, kind="air")
 
 
 # ---------------------------------------------------------------- serialisation

@@ -151,3 +151,19 @@ def test_bytemodel_monotone():
     w = bytemodel.cycle_bytes(stats, 1, 8, "W")
     assert 0 < v < w
     assert bytemodel.solve_bytes(stats, 2, 10) > bytemodel.solve_bytes(stats, 1, 10)
+
+
+def test_air_hierarchy_restriction_is_not_p_transpose():
+    from oracle import amg_oracle as O
+    C = gallery.convection_diffusion_2d(24, peclet=10.0)
+    h = amg_setup.air_solver(C)
+    assert len(h.levels) > 2
+    lvl = h.levels[0]
+    assert (lvl.R - lvl.P.T).count_nonzero() > 0
+    for i, l in enumerate(h.levels[:-1]):
+        assert abs(h.levels[i + 1].A - l.R @ l.A @ l.P).max() < 1e-12
+    W = ("jacobi", {"iterations": 1, "omega": 2 / 3})
+    ml = O.Hierarchy.from_host(h, presmoother=W, postsmoother=W)
+    b = np.random.default_rng(0).standard_normal(C.shape[0])
+    x, it, rr = O.solve_loop(ml, b, tol=1e-10, maxiter=200)
+    assert rr < 1e-10 and it < 60

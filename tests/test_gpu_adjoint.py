@@ -189,3 +189,53 @@ def test_batched_diffusion_gradients_match_central_differences():
         fd_v = (float(L(_dev(B0), _dev(vals0 + h * dv))) - float(L(_dev(B0), _dev(vals0 - h * dv)))) / (2 * h)
     np.testing.assert_allclose(float(torch.sum(gb * _dev(db))), fd_b, rtol=1e-6)
     np.testing.assert_allclose(float(gv.cpu().numpy() @ dv), fd_v, rtol=1e-6)
+
+
+def test_air_convection_diffusion_gradients():
+    """Config 5b (scaled to 64 x 64): upwind convection-diffusion, Peclet 10, 30 degree
+    wind, AIR hierarchy (R != P^T), k = 4 right-hand sides, L = 1/2 ||x - x*||^2 with x from
+    the standalone AIR V-cycle solve in FP64.  The backward solve runs on the explicit
+    transposed hierarchy (A^T, P' = R^T, R' = P^T); dL/db and dL/dvalues match central
+    differences (h = 1e-6) to 1e-6 relative, and dL/db equals A^-T (x - x*)."""
+    n, k = 64, 4
+    C = gallery.convection_diffusion_2d(n, peclet=10.0, angle=np.pi / 6)
+    host = amg_setup.air_solver(C)
+    ml = MultilevelSolver.from_pyamg(host, presmoother=W23, postsmoother=W23)
+    assert ml.transposed() is not ml
+    rng = np.random.default_rng(3)
+    B0 = rng.standard_normal((C.shape[0], k))
+    Xs = _dev(rng.standard_normal((C.shape[0], k)))
+    pattern = CSRMatrix.from_scipy(C)
+    vals0 = C.data.copy()
+
+    def L(Bm, vv):
+        x = ml.solve(Bm, A=SparseA(pattern, vv), tol=1e-13, maxiter=400)
+        return 0.5 * torch.sum((x - Xs) ** 2), x
+
+    Bt = _dev(B0).requires_grad_(True)
+    vt = _dev(vals0).requires_grad_(True)
+    loss, x = L(Bt, vt)
+    gb, gv = torch.autograd.grad(loss, (Bt, vt))
+    lam = np.linalg.solve(C.T.toarray(), (x - Xs).detach().cpu().numpy())
+    np.testing.assert_allclose(gb.cpu().numpy(), lam, rtol=1e-7, atol=1e-10)
+    h = 1e-6
+    db = rng.standard_normal(B0.shape)
+    dv = rng.standard_normal(vals0.shape) * np.abs(vals0)
+    with torch.no_grad():
+        f = lambda Bm, vv: float(L(_dev(Bm), _dev(vv))[0])
+        fd_b = (f(B0 + h * db, vals0) - f(B0 - h * db, vals0)) / (2 * h)
+        fd_v = (f(B0, vals0 + h * dv) - f(B0, vals0 - h * dv)) / (2 * h)
+    np.testing.assert_allclose(float(torch.sum(gb * _dev(db))), fd_b, rtol=1e-6)
+    np.testing.assert_allclose(float(gv.cpu().numpy() @ dv), fd_v, rtol=1e-6)
+
+
+@pytest.mark.parametrize("factory", ["smoothed_aggregation_solver", "ruge_stuben_solver", "air_solver"])
+def test_from_pyamg_compatibility(factory):
+    """tests/test_multilevel.py:322-333 for the factories restated here."""
+    A = gallery.poisson((20, 20))
+    assert len(MultilevelSolver.from_pyamg(getattr(amg_setup, factory)(A), coarse_solver="jacobi").levels) > 1
+    ml = MultilevelSolver.from_pyamg(getattr(amg_setup, factory)(A), presmoother=RHO, postsmoother=RHO,
+                                     coarse_solver="jacobi")
+    b = np.ones(A.shape[0])
+    x = ml.solve(b, tol=1e-8, maxiter=300)
+    assert np.linalg.norm(b - A @ x) < 1e-8 * np.linalg.norm(b)
