@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace amg {
 
 constexpr int kBlock = 256;     // threads per CTA for every grid kernel
@@ -315,37 +317,44 @@ csr_kb(const int* __restrict__ rowptr, const int* __restrict__ col,
         }
       }
       const int cnt = min(G, e - base);
-      for (int t = 0; t < cnt; t += kB) {
-        int cc[kB];
-        A vv[kB];
+      // One batch of NB gathers: NB independent loads in flight, then their FMAs.  Slots
+      // past the row's end gather the batch's first column again (a valid, cached row)
+      // with a zero coefficient, so a batch has no per-slot branches; the padded products
+      // add exactly zero for finite x.
+      auto batch = [&](auto nb, int t) {
+        constexpr int NB = decltype(nb)::value;
+        int cc[NB];
+        A vv[NB];
 #pragma unroll
-        for (int u = 0; u < kB; ++u) {
-          const int src = (t + u < G) ? t + u : 0;
-          cc[u] = __shfl_sync(gmask, c_l, src, G);
-          vv[u] = __shfl_sync(gmask, v_l, src, G);
-          if (t + u >= cnt) vv[u] = A(0);
+        for (int u = 0; u < NB; ++u) {
+          cc[u] = __shfl_sync(gmask, c_l, (t + u) & (G - 1), G);
+          vv[u] = __shfl_sync(gmask, v_l, (t + u) & (G - 1), G);
+          const bool ok = t + u < cnt;
+          vv[u] = ok ? vv[u] : A(0);
+          if (u > 0) cc[u] = ok ? cc[u] : cc[0];
         }
 #pragma unroll
         for (int j = 0; j < NCH; ++j) {
           const int ch = lane + j * G;
           if (ch < nchunks) {
-            A xv[kB][KV];
+            A xv[NB][KV];
 #pragma unroll
-            for (int u = 0; u < kB; ++u) {
-              if (t + u < cnt) {
-                op.template xk<KV>(cc[u], ch * KV, xv[u]);
-              } else {
+            for (int u = 0; u < NB; ++u) op.template xk<KV>(cc[u], ch * KV, xv[u]);
 #pragma unroll
-                for (int v = 0; v < KV; ++v) xv[u][v] = A(0);
-              }
-            }
+            for (int u = 0; u < NB; ++u)
 #pragma unroll
-            for (int u = 0; u < kB; ++u)
-#pragma unroll
-              for (int v = 0; v < KV; ++v) acc[j][v] += vv[u] * xv[u][v];
+              for (int v = 0; v < KV; ++v) acc[j][v] = fma(vv[u], xv[u][v], acc[j][v]);
           }
         }
-      }
+      };
+      // full batches, then the remainder in the smallest batch that holds it
+      int t = 0;
+      for (; t + kB <= cnt; t += kB) batch(std::integral_constant<int, kB>{}, t);
+      const int rem = cnt - t;
+      if (rem > 4) batch(std::integral_constant<int, kB>{}, t);
+      else if (rem > 2) batch(std::integral_constant<int, 4>{}, t);
+      else if (rem == 2) batch(std::integral_constant<int, 2>{}, t);
+      else if (rem == 1) batch(std::integral_constant<int, 1>{}, t);
     }
     // next row's first (col, val) chunk, issued before this row's epilogue
     s = ns;
@@ -363,6 +372,84 @@ csr_kb(const int* __restrict__ rowptr, const int* __restrict__ col,
     }
   }
   if (op.reduces()) block_reduce_k<Op, G, KV, NCH>(op, rc, red);
+}
+
+// k > 1, lean variant with R independent rows in flight per lane group (rows row0,
+// row0 + ngrp, ...; one column chunk per lane, G * KV >= k).  Lanes never exchange data:
+// every lane reads the rows' (col, val) itself (same address across the group, one
+// broadcast access), the first nonzero of every row is gathered together, and the rest of
+// each row runs as a plain loop the compiler unrolls, so its gathers overlap.  No
+// shuffles, no padded slots, and lanes without a column chunk skip the row loop at once:
+// fewer instructions per nonzero than csr_kb.  Products are accumulated in the row's
+// nonzero order with fused multiply-adds, as in csr_kb.
+template <class Op, int G, int KV, int R>
+__global__ void __launch_bounds__(kBlock, 4)
+csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
+       const typename Op::V* __restrict__ val, int n_rows, Op op, RedCtx rc) {
+  count_launch();
+  if (op.stopped()) return;
+  using A = typename Op::Acc;
+  const int lane = threadIdx.x % G;
+  const int grp = (blockIdx.x * kBlock + threadIdx.x) / G;
+  const int ngrp = gridDim.x * (kBlock / G);
+  const int c0 = lane * KV;
+  double red[1][KV];
+#pragma unroll
+  for (int v = 0; v < KV; ++v) red[0][v] = 0.0;
+  if (c0 < rc.k) {
+    for (int row0 = grp; row0 < n_rows; row0 += R * ngrp) {
+      int s[R], e[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int row = row0 + r * ngrp;
+        s[r] = 0;
+        e[r] = 0;
+        if (row < n_rows) {
+          s[r] = __ldg(rowptr + row);
+          e[r] = __ldg(rowptr + row + 1);
+        }
+      }
+      PreT<A, KV> pre[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        if (row0 + r * ngrp < n_rows) op.template prek<KV>(row0 + r * ngrp, c0, pre[r]);
+      // first nonzero of every row, gathered together
+      int c1[R];
+      A a1[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        c1[r] = 0;
+        a1[r] = A(0);
+        if (s[r] < e[r]) {
+          c1[r] = __ldg(col + s[r]);
+          a1[r] = static_cast<A>(__ldg(val + s[r]));
+        }
+      }
+      A acc[R][KV];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        A xv[KV];
+        op.template xk<KV>(c1[r], c0, xv);
+#pragma unroll
+        for (int v = 0; v < KV; ++v) acc[r][v] = (s[r] < e[r]) ? fma(a1[r], xv[v], A(0)) : A(0);
+      }
+      // the rest of every row, then its epilogue
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+#pragma unroll 4
+        for (int nz = s[r] + 1; nz < e[r]; ++nz) {
+          const int cj = __ldg(col + nz);
+          const A a = static_cast<A>(__ldg(val + nz));
+          A xv[KV];
+          op.template xk<KV>(cj, c0, xv);
+#pragma unroll
+          for (int v = 0; v < KV; ++v) acc[r][v] = fma(a, xv[v], acc[r][v]);
+        }
+        if (row0 + r * ngrp < n_rows) op.template epik<KV>(row0 + r * ngrp, c0, acc[r], pre[r], red[0]);
+      }
+    }
+  }
+  if (op.reduces()) block_reduce_k<Op, G, KV, 1>(op, rc, red);
 }
 
 // Elementwise over [n_rows, k] with the same (group, lane, KV, NCH) mapping.

@@ -217,8 +217,12 @@ namespace amg {
 // ------------------------------------------------------------------ launch helpers
 struct Cfg {
   int G = 1, KV = 1, NCH = 1, grid = 1;
+  bool lean = false;  // csr_kr (two rows in flight per lane group, NCH == 1)
   size_t smem = 0;
 };
+
+// A tuned lanes-per-row value of kLeanCode + G selects csr_kr with G lanes.
+constexpr int kLeanCode = 64;
 
 static int pow2ceil(int v) {
   int p = 1;
@@ -258,18 +262,23 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     c.KV = pick_kv<T>(k, ptrs);
     const int nch = k / c.KV;
     c.G = std::max(4, std::min(32, pow2ceil(nch)));
-    if (tune_rowptr) {
-      const int tg = tuned_g(tune_rowptr, tune_nnz, k, int(sizeof(T)), c.KV, tune_tag);
-      if (tg) c.G = tg;
-    }
+    int tg = 0;
+    if (tune_rowptr) tg = tuned_g(tune_rowptr, tune_nnz, k, int(sizeof(T)), c.KV, tune_tag);
     if (const char* fg = std::getenv("AMG_KB_G")) {  // manual override (experiments)
       const int g = atoi(fg);
-      if (g == 4 || g == 8 || g == 16 || g == 32) c.G = g;
+      const int gl = g >= kLeanCode ? g - kLeanCode : g;
+      if (gl == 4 || gl == 8 || gl == 16 || gl == 32) tg = g;
     }
+    if (tg >= kLeanCode) {
+      tg -= kLeanCode;
+      c.lean = true;
+    }
+    if (tg) c.G = tg;
     const int per = (nch + c.G - 1) / c.G;
     if (per > kMaxCh)
       fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);
     c.NCH = per <= 1 ? 1 : per <= 2 ? 2 : 4;
+    if (c.NCH > 1 || c.KV == 1) c.lean = false;
     if (c.KV == 1 && c.NCH > 1) c.G = 32;
     c.smem = sizeof(double) * std::max<size_t>(size_t(kBlock / c.G) * k, kBlock);
   }
@@ -325,8 +334,18 @@ static void launch_k1(const Csr& M, const typename Op::V* vals, const Op& op, co
 template <class Op, int G, int KV, int NCH>
 static void launch_kb(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                       RedCtx rc, cudaStream_t s) {
-  const int grid = cap_grid(csr_kb<Op, G, KV, NCH>, c.grid, c.smem);
-  launch(csr_kb<Op, G, KV, NCH>, grid, kBlock, c.smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+  const size_t smem = op.reduces() ? c.smem : 0;  // the reduction's scratch only
+  const int grid = cap_grid(csr_kb<Op, G, KV, NCH>, c.grid, smem);
+  launch(csr_kb<Op, G, KV, NCH>, grid, kBlock, smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+}
+
+// csr_kr: two rows in flight per lane group, one column chunk per lane.
+template <class Op, int G, int KV>
+static void launch_kr(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
+                      RedCtx rc, cudaStream_t s) {
+  const size_t smem = op.reduces() ? c.smem : 0;  // the reduction's scratch only
+  const int grid = cap_grid(csr_kr<Op, G, KV, 2>, c.grid, smem);
+  launch(csr_kr<Op, G, KV, 2>, grid, kBlock, smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
 }
 
 // (G, NCH) pairs: any G in {4, 8, 16, 32} with NCH in {1, 2, 4} for vector widths >= 2;
@@ -334,6 +353,12 @@ static void launch_kb(const Csr& M, const typename Op::V* vals, const Op& op, co
 template <class Op, int KV, int G>
 static void dispatch_kb_nch(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                             RedCtx rc, cudaStream_t s) {
+  if constexpr (KV >= 2) {
+    if (c.lean) {  // cfg_k sets lean with one chunk per lane only
+      launch_kr<Op, G, KV>(M, vals, op, c, rc, s);
+      return;
+    }
+  }
   if (c.NCH == 1) launch_kb<Op, G, KV, 1>(M, vals, op, c, rc, s);
   else if constexpr (KV >= 2 || G == 32) {
     if (c.NCH == 2) launch_kb<Op, G, KV, 2>(M, vals, op, c, rc, s);
@@ -407,6 +432,9 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
     const int per = (nch + g - 1) / g;
     if (per <= kMaxCh && (kv > 1 || per == 1 || g == 32)) cands.push_back(g);
   }
+  if (kv > 1)  // the lean kernel, one chunk per lane
+    for (int g = 4; g <= gmax; g <<= 1)
+      if (nch <= g) cands.push_back(kLeanCode + g);
   if (cands.size() <= 1) {
     set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, cands.empty() ? gmax : cands[0]);
     return;
@@ -504,8 +532,9 @@ void autotune_cycle(amg_hierarchy* h, Plan* pl, int k, const Csr* A0, cudaStream
 
 template <class Op, int G, int KV, int NCH>
 static void launch_elem(int n, const Op& op, const Cfg& c, RedCtx rc, cudaStream_t s) {
-  const int grid = cap_grid(elem_kb<Op, G, KV, NCH>, c.grid, c.smem);
-  launch(elem_kb<Op, G, KV, NCH>, grid, kBlock, c.smem, s, n, op, rc);
+  const size_t smem = op.reduces() ? c.smem : 0;  // the reduction's scratch only
+  const int grid = cap_grid(elem_kb<Op, G, KV, NCH>, c.grid, smem);
+  launch(elem_kb<Op, G, KV, NCH>, grid, kBlock, smem, s, n, op, rc);
 }
 
 template <class Op, int KV>

@@ -388,7 +388,7 @@ def run_ours(args):
             traffic = json.load(f).get("dram_bytes_per_launch")
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                        "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind + " (burst copy)",
-                       "kernel": "csr_kb<OpJacobi<float,XS_PLAIN>,G,4,NCH> (autotuned layout): fine-level fused "
+                       "kernel": "csr_kb / csr_kr <OpJacobi<float,XS_PLAIN>> (autotuned kernel and layout): fine-level fused "
                                  f"Jacobi sweep, FP32, k={k}, N={Nn}",
                        "algorithmic_bytes_per_launch": jb, "launch_us": t_launch * 1e6}
 
