@@ -38,6 +38,15 @@ __device__ __forceinline__ void count_launch() {
 }
 
 // ------------------------------------------------------------------ vector access
+// Element offset of (row j, column c) in a [rows, ld] array.  Rows, columns and ld are
+// non-negative int32, so one unsigned 32 x 32 -> 64-bit multiply-add forms it (a signed
+// 64-bit product costs more instructions per gathered row).
+__device__ __forceinline__ size_t voff(int j, int ld, int c) {
+  return static_cast<size_t>(static_cast<unsigned long long>(static_cast<unsigned>(j)) * static_cast<unsigned>(ld)) +
+         static_cast<unsigned>(c);
+}
+
+
 template <class T, int KV>
 __device__ __forceinline__ void ld_vec(const T* __restrict__ p, T (&v)[KV]) {
   if constexpr (sizeof(T) * KV == 16) {
@@ -543,10 +552,10 @@ struct XSource {
   template <int KV>
   __device__ __forceinline__ void getk(int j, int c0, T (&v)[KV]) const {
     if constexpr (XS == XS_PLAIN) {
-      ld_vec<T, KV>(x + (size_t)j * ld + c0, v);
+      ld_vec<T, KV>(x + voff(j, ld, c0), v);
     } else if constexpr (XS == XS_JAC0) {
       T bv[KV];
-      ld_vec<T, KV>(b + (size_t)j * ld + c0, bv);
+      ld_vec<T, KV>(b + voff(j, ld, c0), bv);
       const T d = __ldg(dinv + j);
 #pragma unroll
       for (int i = 0; i < KV; ++i) v[i] = omega * (d * bv[i]);
@@ -602,7 +611,7 @@ struct OpJacobi {
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& p) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     xs.template getk<KV>(i, c0, p.x);
     ld_vec<T, KV>(b + o, p.b);
     p.d = __ldg(dinv + i);
@@ -617,7 +626,11 @@ struct OpJacobi {
       const T temp = p.d * r[v] + p.x[v];
       y[v] = (T(1) - omega) * p.x[v] + omega * temp;
     }
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
+    if (!(norm | (rdot64 != nullptr) | (rdot32 != nullptr) | (active != nullptr))) {
+      st_vec<T, KV>(out + o, y);  // the plain sweep: one uniform test per row
+      return;
+    }
     if (norm) {
 #pragma unroll
       for (int v = 0; v < KV; ++v) red[v] += (double)r[v] * (double)r[v];
@@ -680,7 +693,7 @@ struct OpResid {
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& p) const {
-    ld_vec<T, KV>(b + (size_t)i * ld + c0, p.b);
+    ld_vec<T, KV>(b + voff(i, ld, c0), p.b);
   }
   template <int KV>
   __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& p,
@@ -691,12 +704,12 @@ struct OpResid {
       r[v] = p.b[v] - s[v];
       if constexpr (NORM) red[v] += (double)r[v] * (double)r[v];
     }
-    if constexpr (STORE) st_vec<T, KV>(out + (size_t)i * ld + c0, r);
+    if constexpr (STORE) st_vec<T, KV>(out + voff(i, ld, c0), r);
     if (out_lo) {
       TLO rl[KV];
 #pragma unroll
       for (int v = 0; v < KV; ++v) rl[v] = static_cast<TLO>(r[v]);
-      st_vec<TLO, KV>(out_lo + (size_t)i * ld + c0, rl);
+      st_vec<TLO, KV>(out_lo + voff(i, ld, c0), rl);
     }
   }
   __device__ __forceinline__ int finalize_col(int c, double s) const {
@@ -727,7 +740,7 @@ struct OpAxpy {
   __device__ __forceinline__ T x1(int j) const { return __ldg(x + j); }
   template <int KV>
   __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const {
-    ld_vec<T, KV>(x + (size_t)j * ld + c0, v);
+    ld_vec<T, KV>(x + voff(j, ld, c0), v);
   }
   __device__ __forceinline__ double epi1(int i, T s) const {
     out[i] = base.get1(i) + s;
@@ -743,7 +756,7 @@ struct OpAxpy {
     T y[KV];
 #pragma unroll
     for (int v = 0; v < KV; ++v) y[v] = p.x[v] + s[v];
-    st_vec<T, KV>(out + (size_t)i * ld + c0, y);
+    st_vec<T, KV>(out + voff(i, ld, c0), y);
   }
   __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
   __device__ __forceinline__ void finalize_all(int) const {}
@@ -767,7 +780,7 @@ struct OpCgQ {
   __device__ __forceinline__ T x1(int j) const { return __ldg(p + j); }
   template <int KV>
   __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const {
-    ld_vec<T, KV>(p + (size_t)j * ld + c0, v);
+    ld_vec<T, KV>(p + voff(j, ld, c0), v);
   }
   __device__ __forceinline__ double epi1(int i, T s) const {
     if (q) q[i] = s;
@@ -775,14 +788,14 @@ struct OpCgQ {
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
-    ld_vec<T, KV>(p + (size_t)i * ld + c0, pp.x);
+    ld_vec<T, KV>(p + voff(i, ld, c0), pp.x);
   }
   template <int KV>
   __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& pp,
                                        double (&red)[KV]) const {
 #pragma unroll
     for (int v = 0; v < KV; ++v) red[v] += (double)pp.x[v] * (double)s[v];
-    if (q) st_vec<T, KV>(q + (size_t)i * ld + c0, s);
+    if (q) st_vec<T, KV>(q + voff(i, ld, c0), s);
   }
   __device__ __forceinline__ int finalize_col(int c, double s) const {
     alpha[c] = gamma[c] / s;
@@ -814,7 +827,7 @@ struct OpCgUpdA {
   __device__ __forceinline__ T x1(int j) const { return __ldg(p + j); }
   template <int KV>
   __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const {
-    ld_vec<T, KV>(p + (size_t)j * ld + c0, v);
+    ld_vec<T, KV>(p + voff(j, ld, c0), v);
   }
   __device__ __forceinline__ double epi1(int i, T s) const {
     T rv = r[i];
@@ -829,7 +842,7 @@ struct OpCgUpdA {
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     ld_vec<T, KV>(p + o, pp.x);
     ld_vec<T, KV>(x + o, pp.b);
     ld_vec<T, KV>(r + o, pp.c);
@@ -837,7 +850,7 @@ struct OpCgUpdA {
   template <int KV>
   __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& pp,
                                        double (&red)[KV]) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     T xv[KV], rv[KV];
     bool any = false;
 #pragma unroll
@@ -888,7 +901,7 @@ struct OpCgUpdate {
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&red)[KV]) const {
     T xv[KV], rv[KV], pv[KV], qv[KV];
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     ld_vec<T, KV>(r + o, rv);
     bool any = false;
 #pragma unroll
@@ -934,7 +947,7 @@ struct OpCgDir {
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&)[KV]) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     T pv[KV], zv[KV];
     ld_vec<T, KV>(p + o, pv);
     ld_cvt<T, TZ, KV>(z + o, zv);
@@ -959,7 +972,7 @@ struct OpRefine {
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&)[KV]) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     T xv[KV], ev[KV];
     ld_vec<T, KV>(x + o, xv);
     ld_cvt<T, TE, KV>(e + o, ev);
@@ -986,7 +999,7 @@ struct OpJac0 {
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&)[KV]) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     T bv[KV];
     ld_vec<T, KV>(b + o, bv);
     const T d = __ldg(dinv + i);
@@ -1023,7 +1036,7 @@ struct OpSetup {
   __device__ __forceinline__ bool stopped() const { return false; }
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&red)[KV]) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     T v[KV];
     ld_vec<T, KV>(src + o, v);
 #pragma unroll
@@ -1084,7 +1097,7 @@ struct OpMaskCopy {
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&red)[KV]) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     T v[KV];
     ld_vec<T, KV>(src + o, v);
     if constexpr (DOT) {
@@ -1123,7 +1136,7 @@ struct OpConvert {
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&)[KV]) const {
-    const size_t o = (size_t)i * ld + c0;
+    const size_t o = voff(i, ld, c0);
     TD v[KV];
     ld_cvt<TD, TS, KV>(src + o, v);
     st_vec<TD, KV>(dst + o, v);
