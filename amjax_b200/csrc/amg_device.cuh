@@ -762,40 +762,56 @@ struct OpAxpy {
   __device__ __forceinline__ void finalize_all(int) const {}
 };
 
-// CG: q = A p and <p, q> per column; alpha = gamma / <p, q>.
-template <class T>
-struct OpCgQ {
+
+// CG step with the direction update folded in: p_new = z + beta p_old (z in the cycle's
+// type, beta per column from the last cycle) is formed on the fly for every gathered row
+// and written for the row's own entries into the other direction buffer (other rows
+// still gather p_old); <p_new, A p_new> is reduced per column, alpha = gamma / <p, A p>.
+// The gathered and the stored p_new come from the same fused multiply-add, so they are
+// identical.  This replaces the separate pass p = z + beta p before <p, A p>.
+template <class T, class TZ>
+struct OpCgQDir {
   using V = T;
   using Acc = T;
   static constexpr bool kReduce = true;
   __host__ __device__ __forceinline__ bool reduces() const { return kReduce; }
-  const T* p;
-  T* q;
+  const T* p_old;
+  const TZ* z;
+  T* p_new;
+  const double* beta;
   int ld;
   const int* stop;
   const double* gamma;
   double* alpha;
 
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
-  __device__ __forceinline__ T x1(int j) const { return __ldg(p + j); }
+  __device__ __forceinline__ T x1(int j) const {
+    return fma(static_cast<T>(__ldg(beta)), __ldg(p_old + j), static_cast<T>(__ldg(z + j)));
+  }
   template <int KV>
   __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const {
-    ld_vec<T, KV>(p + voff(j, ld, c0), v);
+    const size_t o = voff(j, ld, c0);
+    T pv[KV], zv[KV];
+    ld_vec<T, KV>(p_old + o, pv);
+    ld_cvt<T, TZ, KV>(z + o, zv);
+#pragma unroll
+    for (int i = 0; i < KV; ++i) v[i] = fma(static_cast<T>(__ldg(beta + c0 + i)), pv[i], zv[i]);
   }
   __device__ __forceinline__ double epi1(int i, T s) const {
-    if (q) q[i] = s;
-    return (double)__ldg(p + i) * (double)s;
+    const T pn = x1(i);
+    p_new[i] = pn;
+    return (double)pn * (double)s;
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
-    ld_vec<T, KV>(p + voff(i, ld, c0), pp.x);
+    xk<KV>(i, c0, pp.x);
   }
   template <int KV>
   __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& pp,
                                        double (&red)[KV]) const {
 #pragma unroll
     for (int v = 0; v < KV; ++v) red[v] += (double)pp.x[v] * (double)s[v];
-    if (q) st_vec<T, KV>(q + voff(i, ld, c0), s);
+    st_vec<T, KV>(p_new + voff(i, ld, c0), pp.x);
   }
   __device__ __forceinline__ int finalize_col(int c, double s) const {
     alpha[c] = gamma[c] / s;
@@ -934,30 +950,6 @@ struct OpCgUpdate {
   __device__ __forceinline__ void finalize_all(int any) const { ctl.set_any(any); }
 };
 
-// CG direction: p = z + beta p (z in the cycle's type).
-template <class T, class TZ>
-struct OpCgDir {
-  static constexpr bool kReduce = false;
-  __host__ __device__ __forceinline__ bool reduces() const { return kReduce; }
-  T* p;
-  const TZ* z;
-  const double* beta;
-  int ld;
-  const int* stop;
-  __device__ __forceinline__ bool stopped() const { return stop && *stop; }
-  template <int KV>
-  __device__ __forceinline__ void elem(int i, int c0, double (&)[KV]) const {
-    const size_t o = voff(i, ld, c0);
-    T pv[KV], zv[KV];
-    ld_vec<T, KV>(p + o, pv);
-    ld_cvt<T, TZ, KV>(z + o, zv);
-#pragma unroll
-    for (int v = 0; v < KV; ++v) pv[v] = zv[v] + static_cast<T>(beta[c0 + v]) * pv[v];
-    st_vec<T, KV>(p + o, pv);
-  }
-  __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
-  __device__ __forceinline__ void finalize_all(int) const {}
-};
 
 // Mixed-precision refinement update: x += e for active columns (e in the cycle's type).
 template <class T, class TE>

@@ -167,8 +167,8 @@ struct Plan {
   size_t csize = 8;                   // bytes of the cycle's type
   std::vector<void*> X, B, W1, W2;    // per level, cycle type
   void* r_out = nullptr;              // outer residual (outer type)
-  void* p_out = nullptr;
-  void* q_out = nullptr;
+  void* p_out = nullptr;              // CG direction buffers (outer type): p_out and q_out
+  void* q_out = nullptr;              //   alternate as old / new direction per CG step
   void* r_lo = nullptr;               // cycle-type copy of r (MIXED)
   double* dscal = nullptr;            // per-column doubles: thresh, nr, normb, gamma, alpha, beta
   int* iscal = nullptr;               // per-column ints: active, iters; then stop, gcount
