@@ -68,7 +68,10 @@ void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit*
     tu.x = x; tu.r = r; tu.p = pb; tu.r_lo = mixed ? rc : nullptr;
     tu.alpha = pl->alpha(); tu.active = pl->active(); tu.ld = k; tu.stop = nullptr;
     tu.ctl = make_ctl(pl, maxiter);
-    tune_op(*A0, tu, k, red_of(pl), user, {x, r, pb, tu.r_lo});
+    tune_op(*A0, tu, k, red_of(pl), user, {x, r, pb, tu.r_lo}, [&](cudaStream_t ts) {
+      CK(cudaMemcpyAsync(pl->active(), ones.data(), sizeof(int) * k, cudaMemcpyHostToDevice, ts));
+      CK(cudaStreamSynchronize(ts));
+    });
   }
 }
 

@@ -415,9 +415,13 @@ bool tuning_enabled();
 // Time one fused CSR op (a fully formed instance on scratch buffers, stop flag off) with
 // each candidate lanes-per-row G (each with its chunks per lane) and keep the fastest for
 // this (matrix, k, type, op).  Runs outside stream capture, once per key.
+// `before` (optional) runs ahead of every launch, outside the timed region: it restores
+// state an op's finalisation changes (the CG update freezes columns it judges converged,
+// and frozen columns skip their writes, which would flatter later candidates).
 template <class Op>
 void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
-             std::initializer_list<const void*> ptrs) {
+             std::initializer_list<const void*> ptrs,
+             const std::function<void(cudaStream_t)>& before = {}) {
   using T = typename Op::Acc;
   if (k == 1 || M.n_rows == 0) return;
   if (M.nnz > 0 && !M.template vals<typename Op::V>()) return;
@@ -446,9 +450,11 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
   float best_t = 1e30f;
   for (int g : cands) {
     set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, g);
+    if (before) before(s);
     run_csr(M, op, k, red, s, ptrs);
     float tmin = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
+      if (before) before(s);
       CK(cudaEventRecord(e0, s));
       run_csr(M, op, k, red, s, ptrs);
       CK(cudaEventRecord(e1, s));
