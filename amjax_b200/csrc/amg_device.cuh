@@ -406,6 +406,13 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
 #pragma unroll
   for (int v = 0; v < KV; ++v) red[0][v] = 0.0;
   if (c0 < rc.k) {
+    // gathers: through the op's per-lane prepared form when it has one (kPrepared)
+    Op lop = op;
+    if constexpr (Op::kPrepared) lop.template prepare<KV>(c0);
+    auto gather = [&](int j, A (&v)[KV]) {
+      if constexpr (Op::kPrepared) lop.template xkp<KV>(j, c0, v);
+      else op.template xk<KV>(j, c0, v);
+    };
     for (int row0 = grp; row0 < n_rows; row0 += R * ngrp) {
       int s[R], e[R];
 #pragma unroll
@@ -438,7 +445,7 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         A xv[KV];
-        op.template xk<KV>(c1[r], c0, xv);
+        gather(c1[r], xv);
 #pragma unroll
         for (int v = 0; v < KV; ++v) acc[r][v] = (s[r] < e[r]) ? fma(a1[r], xv[v], A(0)) : A(0);
       }
@@ -450,7 +457,7 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
           const int cj = __ldg(col + nz);
           const A a = static_cast<A>(__ldg(val + nz));
           A xv[KV];
-          op.template xk<KV>(cj, c0, xv);
+          gather(cj, xv);
 #pragma unroll
           for (int v = 0; v < KV; ++v) acc[r][v] = fma(a, xv[v], acc[r][v]);
         }
@@ -575,6 +582,7 @@ struct XSource {
 //   rdot64 / rdot32: also reduce <r, out> per column (the CG's gamma = <r, z>).
 template <class T, int XS>
 struct OpJacobi {
+  static constexpr bool kPrepared = false;
   using V = T;
   using Acc = T;
   XSource<T, XS> xs;
@@ -669,6 +677,7 @@ struct OpJacobi {
 // mixed-precision refinement).  STORE: write r in T.
 template <class T, class VT, int XS, bool STORE, class TLO, bool NORM>
 struct OpResid {
+  static constexpr bool kPrepared = false;
   using V = VT;
   using Acc = T;
   static constexpr bool kReduce = NORM;
@@ -726,6 +735,7 @@ struct OpResid {
 // With base = zero this is the plain SpMV used for restriction R r.
 template <class T, int BS>
 struct OpAxpy {
+  static constexpr bool kPrepared = false;
   using V = T;
   using Acc = T;
   static constexpr bool kReduce = false;
@@ -771,6 +781,7 @@ struct OpAxpy {
 // identical.  This replaces the separate pass p = z + beta p before <p, A p>.
 template <class T, class TZ>
 struct OpCgQDir {
+  static constexpr bool kPrepared = true;
   using V = T;
   using Acc = T;
   static constexpr bool kReduce = true;
@@ -783,10 +794,27 @@ struct OpCgQDir {
   const int* stop;
   const double* gamma;
   double* alpha;
+  T bl[4];  // beta of one lane's column chunk, loaded once by prepare() (csr_kr)
 
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
   __device__ __forceinline__ T x1(int j) const {
     return fma(static_cast<T>(__ldg(beta)), __ldg(p_old + j), static_cast<T>(__ldg(z + j)));
+  }
+  // Kernels whose lanes keep one column chunk (csr_kr) load the chunk's beta once per lane
+  // and gather through xkp, instead of re-loading beta for every gathered row.
+  template <int KV>
+  __device__ __forceinline__ void prepare(int c0) {
+#pragma unroll
+    for (int i = 0; i < KV; ++i) bl[i] = static_cast<T>(__ldg(beta + c0 + i));
+  }
+  template <int KV>
+  __device__ __forceinline__ void xkp(int j, int c0, T (&v)[KV]) const {
+    const size_t o = voff(j, ld, c0);
+    T pv[KV], zv[KV];
+    ld_vec<T, KV>(p_old + o, pv);
+    ld_cvt<T, TZ, KV>(z + o, zv);
+#pragma unroll
+    for (int i = 0; i < KV; ++i) v[i] = fma(bl[i], pv[i], zv[i]);
   }
   template <int KV>
   __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const {
@@ -825,6 +853,7 @@ struct OpCgQDir {
 // <r, r> and apply the CG loop rule.
 template <class T, class TLO>
 struct OpCgUpdA {
+  static constexpr bool kPrepared = false;
   using V = T;
   using Acc = T;
   static constexpr bool kReduce = true;

@@ -43,17 +43,68 @@ bool pdl_enabled() {
 namespace {
 std::mutex g_tune_mu;
 std::map<std::tuple<const void*, int64_t, int, int, int, const void*>, int> g_tune;
+
+// Tuning file (AMG_TUNE_FILE=path): one decision per line, "op-type nnz k es kv G".  Read
+// once; a decision found there is used without timing, and new decisions are appended.
+// The key has no pointers, so a second process (a profiler run, a service restart) reuses
+// the first one's layouts; two matrices with the same op, nnz, k and types share a line.
+using FileKey = std::tuple<std::string, int64_t, int, int, int>;
+std::map<FileKey, int> g_tune_file;
+bool g_tune_file_loaded = false;
+
+const char* tune_file_path() {
+  const char* p = std::getenv("AMG_TUNE_FILE");
+  return (p && p[0]) ? p : nullptr;
+}
+
+void load_tune_file() {  // g_tune_mu held
+  if (g_tune_file_loaded) return;
+  g_tune_file_loaded = true;
+  const char* path = tune_file_path();
+  if (!path) return;
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  char name[512];
+  long long nnz;
+  int k, es, kv, g;
+  while (fscanf(f, "%511s %lld %d %d %d %d", name, &nnz, &k, &es, &kv, &g) == 6)
+    g_tune_file[FileKey(name, nnz, k, es, kv)] = g;
+  fclose(f);
+}
 }  // namespace
 
 int tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  auto it = g_tune.find(std::make_tuple(rowptr, nnz, k, es, kv, tag));
-  return it == g_tune.end() ? 0 : it->second;
+  const auto key = std::make_tuple(rowptr, nnz, k, es, kv, tag);
+  auto it = g_tune.find(key);
+  if (it != g_tune.end()) return it->second;
+  load_tune_file();
+  if (!g_tune_file.empty()) {
+    auto ft = g_tune_file.find(FileKey(static_cast<const OpTag*>(tag)->name, nnz, k, es, kv));
+    if (ft != g_tune_file.end()) {
+      g_tune[key] = ft->second;
+      return ft->second;
+    }
+  }
+  return 0;
 }
 
-void set_tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag, int g) {
+void set_tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag, int g,
+                 bool final) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[std::make_tuple(rowptr, nnz, k, es, kv, tag)] = g;
+  if (!final) return;
+  const char* path = tune_file_path();
+  if (!path) return;
+  load_tune_file();
+  const char* name = static_cast<const OpTag*>(tag)->name;
+  const FileKey fk(name, nnz, k, es, kv);
+  if (g_tune_file.count(fk)) return;
+  g_tune_file[fk] = g;
+  if (FILE* f = fopen(path, "a")) {
+    fprintf(f, "%s %lld %d %d %d %d\n", name, (long long)nnz, k, es, kv, g);
+    fclose(f);
+  }
 }
 
 bool tuning_enabled() {

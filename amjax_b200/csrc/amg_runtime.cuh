@@ -18,6 +18,7 @@
 #include <cstring>
 #include <functional>
 #include <type_traits>
+#include <typeinfo>
 #include <list>
 #include <map>
 #include <memory>
@@ -241,12 +242,17 @@ static int pick_kv(int k, std::initializer_list<const void*> ptrs) {
 }
 
 // Autotuned lanes-per-row for a (matrix, k, value size, vector width, op type): 0 when
-// untuned.  op_tag<Op>() is a process-wide unique address per op type.
+// untuned.  op_tag<Op>() is a process-wide unique address per op type; it points at the
+// type's name, which keys the optional tuning file (AMG_TUNE_FILE) across processes.
 int tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag);
+
+struct OpTag {
+  const char* name;
+};
 
 template <class Op>
 const void* op_tag() {
-  static const char tag = 0;
+  static const OpTag tag{typeid(Op).name()};
   return &tag;
 }
 
@@ -409,7 +415,9 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
 
 // ------------------------------------------------------------------ autotuner
 // Record the fastest lanes-per-row for (matrix, k, value size, vector width, op type).
-void set_tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag, int g);
+// `final`: the tuner's decision (recorded in AMG_TUNE_FILE when set), not a candidate.
+void set_tuned_g(const void* rowptr, int64_t nnz, int k, int es, int kv, const void* tag, int g,
+                 bool final = false);
 bool tuning_enabled();
 
 // Time one fused CSR op (a fully formed instance on scratch buffers, stop flag off) with
@@ -440,7 +448,7 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
     for (int g = 4; g <= gmax; g <<= 1)
       if (nch <= g) cands.push_back(kLeanCode + g);
   if (cands.size() <= 1) {
-    set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, cands.empty() ? gmax : cands[0]);
+    set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, cands.empty() ? gmax : cands[0], true);
     return;
   }
   cudaEvent_t e0, e1;
@@ -470,7 +478,7 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, best);
+  set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, best, true);
   if (std::getenv("AMG_TUNE_LOG"))
     fprintf(stderr, "[amg tune] rows=%d nnz=%lld k=%d es=%d kv=%d op=%p -> G=%d (%.1f us)\n", M.n_rows,
             (long long)M.nnz, k, int(sizeof(T)), kv, tag, best, best_t * 1e3f);
