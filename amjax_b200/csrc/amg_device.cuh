@@ -47,9 +47,35 @@ __device__ __forceinline__ size_t voff(int j, int ld, int c) {
 }
 
 
+// 32-byte accesses (sm_100: one 256-bit load or store per thread), used by the wide lean
+// kernel; the address must be 32-byte aligned (the launch configuration checks every
+// pointer and the row stride).  The load takes the read-only path: every CSR-op operand
+// it serves is either never written by the kernel or read by its owner before it writes it.
+__device__ __forceinline__ void ld32(const float* p, float* v) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+      : "l"(p));
+}
+__device__ __forceinline__ void ld32(const double* p, double* v) {
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+__device__ __forceinline__ void st32(float* p, const float* v) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+               "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void st32(double* p, const double* v) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
+               : "memory");
+}
+
 template <class T, int KV>
 __device__ __forceinline__ void ld_vec(const T* __restrict__ p, T (&v)[KV]) {
-  if constexpr (sizeof(T) * KV == 16) {
+  if constexpr (sizeof(T) * KV >= 32 && (sizeof(T) * KV) % 32 == 0) {
+    constexpr int n = 32 / sizeof(T);
+#pragma unroll
+    for (int h = 0; h < KV; h += n) ld32(p + h, v + h);
+  } else if constexpr (sizeof(T) * KV == 16) {
     if constexpr (sizeof(T) == 8) {
       double2 t = *reinterpret_cast<const double2*>(p); v[0] = t.x; v[1] = t.y;
     } else {
@@ -65,7 +91,11 @@ __device__ __forceinline__ void ld_vec(const T* __restrict__ p, T (&v)[KV]) {
 
 template <class T, int KV>
 __device__ __forceinline__ void st_vec(T* __restrict__ p, const T (&v)[KV]) {
-  if constexpr (sizeof(T) * KV == 16) {
+  if constexpr (sizeof(T) * KV >= 32 && (sizeof(T) * KV) % 32 == 0) {
+    constexpr int n = 32 / sizeof(T);
+#pragma unroll
+    for (int h = 0; h < KV; h += n) st32(p + h, v + h);
+  } else if constexpr (sizeof(T) * KV == 16) {
     if constexpr (sizeof(T) == 8) {
       *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
     } else {
@@ -794,7 +824,7 @@ struct OpCgQDir {
   const int* stop;
   const double* gamma;
   double* alpha;
-  T bl[4];  // beta of one lane's column chunk, loaded once by prepare() (csr_kr)
+  T bl[8];  // beta of one lane's column chunk, loaded once by prepare() (csr_kr)
 
   __device__ __forceinline__ bool stopped() const { return stop && *stop; }
   __device__ __forceinline__ T x1(int j) const {

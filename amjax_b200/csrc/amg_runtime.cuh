@@ -219,11 +219,25 @@ namespace amg {
 struct Cfg {
   int G = 1, KV = 1, NCH = 1, grid = 1;
   bool lean = false;  // csr_kr (two rows in flight per lane group, NCH == 1)
+  bool wide = false;  // csr_kr with 32-byte vectors (KV = 32 / value size)
   size_t smem = 0;
 };
 
-// A tuned lanes-per-row value of kLeanCode + G selects csr_kr with G lanes.
+// A tuned lanes-per-row value of kLeanCode + G selects csr_kr with G lanes; kWideCode + G
+// selects csr_kr with G lanes of 32-byte vectors.
 constexpr int kLeanCode = 64;
+constexpr int kWideCode = 128;
+
+// Vector width of the wide kernel when every pointer is 32-byte aligned and k is a
+// multiple of it (the row stride is k), else 0.
+template <class T>
+static int wide_kv(int k, std::initializer_list<const void*> ptrs) {
+  const int kv = 32 / int(sizeof(T));
+  if (k % kv != 0) return 0;
+  for (const void* p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) % 32 != 0) return 0;
+  return kv;
+}
 
 static int pow2ceil(int v) {
   int p = 1;
@@ -272,19 +286,28 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     if (tune_rowptr) tg = tuned_g(tune_rowptr, tune_nnz, k, int(sizeof(T)), c.KV, tune_tag);
     if (const char* fg = std::getenv("AMG_KB_G")) {  // manual override (experiments)
       const int g = atoi(fg);
-      const int gl = g >= kLeanCode ? g - kLeanCode : g;
+      const int gl = g >= kWideCode ? g - kWideCode : g >= kLeanCode ? g - kLeanCode : g;
       if (gl == 4 || gl == 8 || gl == 16 || gl == 32) tg = g;
     }
-    if (tg >= kLeanCode) {
+    if (!tune_rowptr) tg %= kLeanCode;  // elementwise passes: lanes only (no lean / wide kernels)
+    if (tg >= kWideCode) {
+      tg -= kWideCode;
+      const int wk = wide_kv<T>(k, ptrs);
+      if (wk && k / wk <= tg) {  // one 32-byte chunk per lane
+        c.KV = wk;
+        c.wide = true;
+      }
+      c.lean = true;
+    } else if (tg >= kLeanCode) {
       tg -= kLeanCode;
       c.lean = true;
     }
     if (tg) c.G = tg;
-    const int per = (nch + c.G - 1) / c.G;
+    const int per = (k / c.KV + c.G - 1) / c.G;
     if (per > kMaxCh)
       fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);
     c.NCH = per <= 1 ? 1 : per <= 2 ? 2 : 4;
-    if (c.NCH > 1 || c.KV == 1) c.lean = false;
+    if (c.NCH > 1 || c.KV == 1) c.lean = c.wide = false;
     if (c.KV == 1 && c.NCH > 1) c.G = 32;
     c.smem = sizeof(double) * std::max<size_t>(size_t(kBlock / c.G) * k, kBlock);
   }
@@ -345,13 +368,16 @@ static void launch_kb(const Csr& M, const typename Op::V* vals, const Op& op, co
   launch(csr_kb<Op, G, KV, NCH>, grid, kBlock, smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
 }
 
-// csr_kr: two rows in flight per lane group, one column chunk per lane.
+// csr_kr: one column chunk per lane; two rows in flight per lane group with 16-byte
+// vectors, one with 32-byte vectors (half the lanes per row, so a warp already holds twice
+// the rows; a second row per group would spill).
 template <class Op, int G, int KV>
 static void launch_kr(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                       RedCtx rc, cudaStream_t s) {
+  constexpr int R = (KV * sizeof(typename Op::Acc) >= 32) ? 1 : 2;
   const size_t smem = op.reduces() ? c.smem : 0;  // the reduction's scratch only
-  const int grid = cap_grid(csr_kr<Op, G, KV, 2>, c.grid, smem);
-  launch(csr_kr<Op, G, KV, 2>, grid, kBlock, smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+  const int grid = cap_grid(csr_kr<Op, G, KV, R>, c.grid, smem);
+  launch(csr_kr<Op, G, KV, R>, grid, kBlock, smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
 }
 
 // (G, NCH) pairs: any G in {4, 8, 16, 32} with NCH in {1, 2, 4} for vector widths >= 2;
@@ -404,6 +430,14 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
       case 16: launch_k1<Op, 16>(M, vals, op, c, rc, s); break;
       default: launch_k1<Op, 32>(M, vals, op, c, rc, s); break;
     }
+  } else if (c.wide) {
+    constexpr int KW = 32 / int(sizeof(typename Op::Acc));
+    switch (c.G) {
+      case 4: launch_kr<Op, 4, KW>(M, vals, op, c, rc, s); break;
+      case 8: launch_kr<Op, 8, KW>(M, vals, op, c, rc, s); break;
+      case 16: launch_kr<Op, 16, KW>(M, vals, op, c, rc, s); break;
+      default: launch_kr<Op, 32, KW>(M, vals, op, c, rc, s); break;
+    }
   } else {
     if (c.KV == 1) dispatch_kb_g<Op, 1>(M, vals, op, c, rc, s);
     else if (c.KV == 2) dispatch_kb_g<Op, 2>(M, vals, op, c, rc, s);
@@ -447,6 +481,9 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
   if (kv > 1)  // the lean kernel, one chunk per lane
     for (int g = 4; g <= gmax; g <<= 1)
       if (nch <= g) cands.push_back(kLeanCode + g);
+  if (const int wk = wide_kv<T>(k, ptrs))  // the wide lean kernel, one 32-byte chunk per lane
+    for (int g = 4; g <= 32; g <<= 1)
+      if (k / wk <= g && g < 2 * std::max(4, pow2ceil(k / wk))) cands.push_back(kWideCode + g);
   if (cands.size() <= 1) {
     set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, cands.empty() ? gmax : cands[0], true);
     return;
