@@ -443,6 +443,10 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
       if constexpr (Op::kPrepared) lop.template xkp<KV>(j, c0, v);
       else op.template xk<KV>(j, c0, v);
     };
+    // The row loop is instantiated twice: with the column sums live (ops that reduce), and
+    // without (the epilogue's sums go to a dead local), so a plain sweep keeps no FP64
+    // accumulators in registers across rows.
+    auto rows = [&](auto reducing) {
     for (int row0 = grp; row0 < n_rows; row0 += R * ngrp) {
       int s[R], e[R];
 #pragma unroll
@@ -491,9 +495,21 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
 #pragma unroll
           for (int v = 0; v < KV; ++v) acc[r][v] = fma(a, xv[v], acc[r][v]);
         }
-        if (row0 + r * ngrp < n_rows) op.template epik<KV>(row0 + r * ngrp, c0, acc[r], pre[r], red[0]);
+        if (row0 + r * ngrp < n_rows) {
+          if constexpr (decltype(reducing)::value) {
+            op.template epik<KV>(row0 + r * ngrp, c0, acc[r], pre[r], red[0]);
+          } else {
+            double unused[KV];
+#pragma unroll
+            for (int v = 0; v < KV; ++v) unused[v] = 0.0;
+            op.template epik<KV>(row0 + r * ngrp, c0, acc[r], pre[r], unused);
+          }
+        }
       }
     }
+    };
+    if (op.reduces()) rows(std::true_type{});
+    else rows(std::false_type{});
   }
   if (op.reduces()) block_reduce_k<Op, G, KV, 1>(op, rc, red);
 }
