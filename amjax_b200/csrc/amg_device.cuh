@@ -421,8 +421,23 @@ csr_kb(const int* __restrict__ rowptr, const int* __restrict__ col,
 // shuffles, no padded slots, and lanes without a column chunk skip the row loop at once:
 // fewer instructions per nonzero than csr_kb.  Products are accumulated in the row's
 // nonzero order with fused multiply-adds, as in csr_kb.
+// Ops whose every launch reduces columns (a compile-time kReduce that is true).
+template <class Op, class = void>
+struct always_reduces : std::false_type {};
+template <class Op>
+struct always_reduces<Op, std::void_t<decltype(Op::kReduce)>> : std::bool_constant<Op::kReduce> {};
+
+// CTAs per SM the registers are sized for: 4 (64 registers), except FP64 ops with 32-byte
+// vectors that always reduce (the CG steps): 3 (85 registers), since their row operands
+// and FP64 column sums spill at 64 (measured: CG update 139 -> 132 us, <p, A p> 110 -> 98 us
+// at N = 250,000, k = 64; the plain FP64 sweep is faster at 4).
+template <class Op, int KV>
+constexpr int kr_min_blocks() {
+  return (KV * sizeof(typename Op::Acc) >= 32 && sizeof(typename Op::Acc) == 8 && always_reduces<Op>::value) ? 3 : 4;
+}
+
 template <class Op, int G, int KV, int R>
-__global__ void __launch_bounds__(kBlock, 4)
+__global__ void __launch_bounds__(kBlock, kr_min_blocks<Op, KV>())
 csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
        const typename Op::V* __restrict__ val, int n_rows, Op op, RedCtx rc) {
   count_launch();
