@@ -421,23 +421,31 @@ csr_kb(const int* __restrict__ rowptr, const int* __restrict__ col,
 // shuffles, no padded slots, and lanes without a column chunk skip the row loop at once:
 // fewer instructions per nonzero than csr_kb.  Products are accumulated in the row's
 // nonzero order with fused multiply-adds, as in csr_kb.
-// Ops whose every launch reduces columns (a compile-time kReduce that is true).
+// Ops whose launches always / never reduce columns (a compile-time kReduce); ops without
+// one decide per launch (the Jacobi sweep's norm and dot are run-time flags).
 template <class Op, class = void>
 struct always_reduces : std::false_type {};
 template <class Op>
 struct always_reduces<Op, std::void_t<decltype(Op::kReduce)>> : std::bool_constant<Op::kReduce> {};
+template <class Op, class = void>
+struct never_reduces : std::false_type {};
+template <class Op>
+struct never_reduces<Op, std::void_t<decltype(Op::kReduce)>> : std::bool_constant<!Op::kReduce> {};
 
-// CTAs per SM the registers are sized for: 4 (64 registers), except FP64 ops with 32-byte
-// vectors that always reduce (the CG steps): 3 (85 registers), since their row operands
-// and FP64 column sums spill at 64 (measured: CG update 139 -> 132 us, <p, A p> 110 -> 98 us
-// at N = 250,000, k = 64; the plain FP64 sweep is faster at 4).
-template <class Op, int KV>
+// CTAs per SM the registers are sized for: 4 (64 registers), except launches that reduce
+// columns with 32-byte vectors: 3 (85 registers), since their row operands and FP64
+// column sums spill at 64 (measured at N = 250,000, k = 64: FP64 CG update 139 -> 132 us,
+// <p, A p> 110 -> 98 us; the plain sweeps are faster at 4).
+template <class Op, int KV, bool RED>
 constexpr int kr_min_blocks() {
-  return (KV * sizeof(typename Op::Acc) >= 32 && sizeof(typename Op::Acc) == 8 && always_reduces<Op>::value) ? 3 : 4;
+  return (RED && KV * sizeof(typename Op::Acc) >= 32) ? 3 : 4;
 }
 
-template <class Op, int G, int KV, int R>
-__global__ void __launch_bounds__(kBlock, kr_min_blocks<Op, KV>())
+// RED: this launch reduces columns (op.reduces(), chosen by the launcher).  The reducing
+// row loop carries the FP64 column sums; the plain one sends the epilogue's sums to a dead
+// local, so a plain sweep keeps no FP64 accumulators in registers across rows.
+template <class Op, int G, int KV, int R, bool RED>
+__global__ void __launch_bounds__(kBlock, kr_min_blocks<Op, KV, RED>())
 csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
        const typename Op::V* __restrict__ val, int n_rows, Op op, RedCtx rc) {
   count_launch();
@@ -458,9 +466,6 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
       if constexpr (Op::kPrepared) lop.template xkp<KV>(j, c0, v);
       else op.template xk<KV>(j, c0, v);
     };
-    // The row loop is instantiated twice: with the column sums live (ops that reduce), and
-    // without (the epilogue's sums go to a dead local), so a plain sweep keeps no FP64
-    // accumulators in registers across rows.
     auto rows = [&](auto reducing) {
     for (int row0 = grp; row0 < n_rows; row0 += R * ngrp) {
       int s[R], e[R];
@@ -523,10 +528,17 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
       }
     }
     };
-    if (op.reduces()) rows(std::true_type{});
-    else rows(std::false_type{});
+    // RED launches run the reducing loop alone; the others keep both loops behind the
+    // run-time test (measured: the plain wide sweep is faster compiled this way, 41.6 vs
+    // 44.9 us, with the same 64-register budget).
+    if constexpr (RED) {
+      rows(std::true_type{});
+    } else {
+      if (op.reduces()) rows(std::true_type{});
+      else rows(std::false_type{});
+    }
   }
-  if (op.reduces()) block_reduce_k<Op, G, KV, 1>(op, rc, red);
+  if (RED || op.reduces()) block_reduce_k<Op, G, KV, 1>(op, rc, red);
 }
 
 // Elementwise over [n_rows, k] with the same (group, lane, KV, NCH) mapping.

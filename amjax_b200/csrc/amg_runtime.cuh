@@ -375,9 +375,17 @@ template <class Op, int G, int KV>
 static void launch_kr(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
                       RedCtx rc, cudaStream_t s) {
   constexpr int R = (KV * sizeof(typename Op::Acc) >= 32) ? 1 : 2;
-  const size_t smem = op.reduces() ? c.smem : 0;  // the reduction's scratch only
-  const int grid = cap_grid(csr_kr<Op, G, KV, R>, c.grid, smem);
-  launch(csr_kr<Op, G, KV, R>, grid, kBlock, smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+  if constexpr (!never_reduces<Op>::value) {
+    if (op.reduces()) {
+      const int grid = cap_grid(csr_kr<Op, G, KV, R, true>, c.grid, c.smem);
+      launch(csr_kr<Op, G, KV, R, true>, grid, kBlock, c.smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+      return;
+    }
+  }
+  if constexpr (!always_reduces<Op>::value) {
+    const int grid = cap_grid(csr_kr<Op, G, KV, R, false>, c.grid, 0);
+    launch(csr_kr<Op, G, KV, R, false>, grid, kBlock, 0, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+  }
 }
 
 // (G, NCH) pairs: any G in {4, 8, 16, 32} with NCH in {1, 2, 4} for vector widths >= 2;
