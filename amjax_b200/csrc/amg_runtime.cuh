@@ -287,9 +287,9 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     if (const char* fg = std::getenv("AMG_KB_G")) {  // manual override (experiments)
       const int g = atoi(fg);
       const int gl = g >= kWideCode ? g - kWideCode : g >= kLeanCode ? g - kLeanCode : g;
-      if (gl == 4 || gl == 8 || gl == 16 || gl == 32) tg = g;
+      if (gl == 4 || gl == 8 || gl == 16 || gl == 32 || (g >= kLeanCode && (gl == 1 || gl == 2))) tg = g;
     }
-    if (!tune_rowptr) tg %= kLeanCode;  // elementwise passes: lanes only (no lean / wide kernels)
+    if (!tune_rowptr && tg >= kLeanCode) tg = 0;  // elementwise passes: no lean / wide kernels
     if (tg >= kWideCode) {
       tg -= kWideCode;
       const int wk = wide_kv<T>(k, ptrs);
@@ -303,6 +303,10 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
       c.lean = true;
     }
     if (tg) c.G = tg;
+    if (c.lean && !c.wide && (k / c.KV + c.G - 1) / c.G > 1) {  // lean needs one chunk per lane
+      c.lean = false;
+      c.G = std::max(4, std::min(32, pow2ceil(nch)));
+    }
     const int per = (k / c.KV + c.G - 1) / c.G;
     if (per > kMaxCh)
       fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);
@@ -441,10 +445,22 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
   } else if (c.wide) {
     constexpr int KW = 32 / int(sizeof(typename Op::Acc));
     switch (c.G) {
+      case 1: launch_kr<Op, 1, KW>(M, vals, op, c, rc, s); break;
+      case 2: launch_kr<Op, 2, KW>(M, vals, op, c, rc, s); break;
       case 4: launch_kr<Op, 4, KW>(M, vals, op, c, rc, s); break;
       case 8: launch_kr<Op, 8, KW>(M, vals, op, c, rc, s); break;
       case 16: launch_kr<Op, 16, KW>(M, vals, op, c, rc, s); break;
       default: launch_kr<Op, 32, KW>(M, vals, op, c, rc, s); break;
+    }
+  } else if (c.lean && c.G < 4) {  // lean kernel with 1 or 2 lanes per row (few columns)
+    if (c.KV == 2) {
+      if (c.G == 1) launch_kr<Op, 1, 2>(M, vals, op, c, rc, s);
+      else launch_kr<Op, 2, 2>(M, vals, op, c, rc, s);
+    } else if constexpr (sizeof(typename Op::Acc) == 4) {
+      if (c.G == 1) launch_kr<Op, 1, 4>(M, vals, op, c, rc, s);
+      else launch_kr<Op, 2, 4>(M, vals, op, c, rc, s);
+    } else {
+      fail(AMG_ERR_INVALID_ARG, "internal: lean layout G=%d KV=%d", c.G, c.KV);
     }
   } else {
     if (c.KV == 1) dispatch_kb_g<Op, 1>(M, vals, op, c, rc, s);
@@ -486,12 +502,14 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
     const int per = (nch + g - 1) / g;
     if (per <= kMaxCh && (kv > 1 || per == 1 || g == 32)) cands.push_back(g);
   }
-  if (kv > 1)  // the lean kernel, one chunk per lane
-    for (int g = 4; g <= gmax; g <<= 1)
-      if (nch <= g) cands.push_back(kLeanCode + g);
+  if (kv > 1)  // the lean kernel, one chunk per lane (1 or 2 lanes per row for few columns)
+    for (int g = 1; g <= gmax; g <<= 1)
+      if (nch <= g && (g >= 4 || kv * int(sizeof(T)) == 16 || kv * int(sizeof(T)) == 8))
+        cands.push_back(kLeanCode + g);
   if (const int wk = wide_kv<T>(k, ptrs))  // the wide lean kernel, one 32-byte chunk per lane
-    for (int g = 4; g <= 32; g <<= 1)
-      if (k / wk <= g && g < 2 * std::max(4, pow2ceil(k / wk))) cands.push_back(kWideCode + g);
+    for (int g = 1; g <= 32; g <<= 1)
+      if (k / wk <= g && g < 2 * std::max(4, pow2ceil(k / wk)) && (g >= 4 || g == pow2ceil(k / wk)))
+        cands.push_back(kWideCode + g);
   if (cands.size() <= 1) {
     set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, cands.empty() ? gmax : cands[0], true);
     return;
