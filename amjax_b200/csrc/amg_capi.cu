@@ -42,7 +42,7 @@ static void jacobi_impl(const amg_csr* Ad, const void* x, const void* b, const v
   if (iterations > 1) CK(cudaMallocAsync(reinterpret_cast<void**>(&tmp), bytes, s));
   try {
     const T* in = static_cast<const T*>(x);
-    if (k > 1) {  // pick the layout once per (matrix, k, type); tuning writes only `out`
+    {  // pick the layout once per (matrix, k, type); tuning writes only `out`
       OpJacobi<T, XS_PLAIN> top{};
       top.xs = XSource<T, XS_PLAIN>{in, static_cast<const T*>(b), static_cast<const T*>(dinv), T(omega), k};
       top.b = static_cast<const T*>(b);

@@ -59,7 +59,7 @@ void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit*
     step(cs, pb, pa);
   };
   autotune_cycle<TC>(h, pl, k, nullptr, user);
-  if (k > 1) {  // the outer CG ops, on scratch (the prologue resets every state they touch)
+  {  // the outer CG ops, on scratch (the prologue resets every state they touch)
     std::vector<int> ones(size_t(k), 1);
     CK(cudaMemcpy(pl->active(), ones.data(), sizeof(int) * k, cudaMemcpyHostToDevice));
     OpCgQDir<TO, TC> tq{pa, z, pb, pl->beta(), k, nullptr, pl->gamma(), pl->alpha()};

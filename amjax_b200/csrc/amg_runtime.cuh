@@ -278,6 +278,10 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
   if (k == 1) {
     c.G = g1;
     c.KV = 1;
+    if (tune_rowptr) {  // autotuned lanes per row (1..32), when the tuner has run
+      const int tg = tuned_g(tune_rowptr, tune_nnz, 1, int(sizeof(T)), 1, tune_tag);
+      if (tg == 1 || tg == 2 || tg == 4 || tg == 8 || tg == 16 || tg == 32) c.G = tg;
+    }
   } else {
     c.KV = pick_kv<T>(k, ptrs);
     const int nch = k / c.KV;
@@ -489,24 +493,26 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
              std::initializer_list<const void*> ptrs,
              const std::function<void(cudaStream_t)>& before = {}) {
   using T = typename Op::Acc;
-  if (k == 1 || M.n_rows == 0) return;
+  if (M.n_rows == 0) return;
   if (M.nnz > 0 && !M.template vals<typename Op::V>()) return;
-  const int kv = pick_kv<T>(k, ptrs);
+  const int kv = k == 1 ? 1 : pick_kv<T>(k, ptrs);
   if (!tuning_enabled()) return;
   const void* tag = op_tag<Op>();
   if (tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag)) return;
   const int nch = k / kv;
   const int gmax = std::max(4, std::min(32, pow2ceil(nch)));
   std::vector<int> cands;
-  for (int g = 4; g <= gmax; g <<= 1) {
+  if (k == 1)  // csr_k1: lanes sharing a row's nonzeros
+    for (int g = 1; g <= 32; g <<= 1) cands.push_back(g);
+  for (int g = 4; g <= gmax && k > 1; g <<= 1) {
     const int per = (nch + g - 1) / g;
     if (per <= kMaxCh && (kv > 1 || per == 1 || g == 32)) cands.push_back(g);
   }
-  if (kv > 1)  // the lean kernel, one chunk per lane (1 or 2 lanes per row for few columns)
+  if (kv > 1 && k > 1)  // the lean kernel, one chunk per lane (1 or 2 lanes per row for few columns)
     for (int g = 1; g <= gmax; g <<= 1)
       if (nch <= g && (g >= 4 || kv * int(sizeof(T)) == 16 || kv * int(sizeof(T)) == 8))
         cands.push_back(kLeanCode + g);
-  if (const int wk = wide_kv<T>(k, ptrs))  // the wide lean kernel, one 32-byte chunk per lane
+  if (const int wk = k > 1 ? wide_kv<T>(k, ptrs) : 0)  // the wide lean kernel, one 32-byte chunk per lane
     for (int g = 1; g <= 32; g <<= 1)
       if (k / wk <= g && g < 2 * std::max(4, pow2ceil(k / wk)) && (g >= 4 || g == pow2ceil(k / wk)))
         cands.push_back(kWideCode + g);
@@ -551,7 +557,6 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
 // prolongation) for this plan's k; level 0 uses A0 when given.
 template <class T>
 void autotune_cycle(amg_hierarchy* h, Plan* pl, int k, const Csr* A0, cudaStream_t s) {
-  if (k == 1) return;
   const int L = int(h->levels.size());
   for (int l = 0; l < L - 1; ++l) {
     const Level& lv = h->levels[l];
