@@ -754,7 +754,9 @@ struct Cycle {
     op.ld = k;
     op.stop = NORM ? nullptr : stop;
     op.ctl = ctl;
-    run_csr(Aof(l), op, k, red, s, {xp, b, out});
+    // every array the op reads picks the vector width (a Jacobi-from-zero source reads
+    // op.xs.b, which at level 0 may be the caller's right-hand side)
+    run_csr(Aof(l), op, k, red, s, {xp, op.xs.b, b, out});
   }
 
   template <int BS>
@@ -765,7 +767,7 @@ struct Cycle {
     op.out = out;
     op.ld = k;
     op.stop = stop;
-    run_csr(M, op, k, red, s, {base, x, out});
+    run_csr(M, op, k, red, s, {base, op.base.b, x, out});
   }
 
   // Level 0 without a post-smoother but with a mask or a fused CG dot: finish with an
