@@ -167,3 +167,10 @@ def test_air_hierarchy_restriction_is_not_p_transpose():
     b = np.random.default_rng(0).standard_normal(C.shape[0])
     x, it, rr = O.solve_loop(ml, b, tol=1e-10, maxiter=200)
     assert rr < 1e-10 and it < 60
+
+
+def test_spectral_radius_on_device_needs_a_cuda_matrix():
+    import scipy.sparse as sp_
+    A = sp_.diags([2.0, 2.0, 2.0]).tocsr()
+    with pytest.raises(ValueError):
+        approximate_spectral_radius(A, np.full(3, 0.5), on_device=True)

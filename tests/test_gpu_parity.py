@@ -218,3 +218,18 @@ def test_launch_counter_counts():
     before = N.kernel_launch_count()
     ml.solve(np.ones(host.levels[0].A.shape[0]), tol=1e-8, maxiter=20)
     assert N.kernel_launch_count() > before
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_spectral_radius_on_device_matches_host(dtype):
+    """The GPU power iteration (same start vector, same 15 steps) agrees with the host
+    estimate the reference's set-up uses (relaxation.py:101-132) to rounding."""
+    from amjax_b200.relaxation.relaxation import approximate_spectral_radius
+    from amjax_b200 import gallery
+    A = CSRMatrix.from_scipy(gallery.poisson((60, 70)), dtype=dtype)
+    Dinv = inverse_diagonal(A)
+    host = approximate_spectral_radius(A, Dinv)
+    dev = approximate_spectral_radius(A, Dinv, on_device=True)
+    tol = 1e-12 if dtype == np.float64 else 1e-5
+    assert abs(dev - host) <= tol * host
+    assert abs(O.approximate_spectral_radius(A.to_scipy(), O.inverse_diagonal(A.to_scipy())) - dev) <= tol * host
