@@ -59,6 +59,23 @@ void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit*
     step(cs, pb, pa);
   };
   autotune_cycle<TC>(h, pl, k, nullptr, user);
+  if (h->levels.size() > 1 && h->levels[0].post.on()) {
+    // the fine post-smoothing sweep with the fused <r, z>: a reducing launch, tuned on its
+    // own (scratch: W1 -> W2 on level 0; the prologue recomputes gamma and zeroes beta)
+    const Level& l0 = h->levels[0];
+    if (const TC* dv = l0.template dinv<TC>()) {
+      TC* w1 = static_cast<TC*>(pl->W1[0]);
+      TC* w2 = static_cast<TC*>(pl->W2[0]);
+      const TC om = TC(l0.post.omega);
+      OpJacobi<TC, XS_PLAIN> op{};
+      op.xs = XSource<TC, XS_PLAIN>{w1, rc, dv, om, k};
+      op.b = rc; op.dinv = dv; op.omega = om; op.out = w2; op.ld = k;
+      op.rdot64 = sizeof(TO) == 8 ? reinterpret_cast<const double*>(r) : nullptr;
+      op.rdot32 = sizeof(TO) == 8 ? nullptr : reinterpret_cast<const float*>(r);
+      op.gamma = pl->gamma(); op.beta = pl->beta();
+      tune_op(*A0, op, k, red_of(pl), user, {w1, rc, w2, r});
+    }
+  }
   {  // the outer CG ops, on scratch (the prologue resets every state they touch)
     std::vector<int> ones(size_t(k), 1);
     CK(cudaMemcpy(pl->active(), ones.data(), sizeof(int) * k, cudaMemcpyHostToDevice));

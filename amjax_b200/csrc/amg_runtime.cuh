@@ -270,16 +270,31 @@ const void* op_tag() {
   return &tag;
 }
 
+// Launches of an op that reduces columns only sometimes (the Jacobi sweep's norm and dot
+// are run-time flags) run a different instantiation (its own register budget), so they
+// are tuned under their own key; untuned, they fall back to the op's plain key.
+template <class Op>
+struct ReducingLaunch {};
+template <class Op>
+const void* op_tag_for(const Op& op) {
+  if constexpr (!always_reduces<Op>::value && !never_reduces<Op>::value) {
+    if (op.reduces()) return op_tag<ReducingLaunch<Op>>();
+  }
+  return op_tag<Op>();
+}
+
 template <class T>
 static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> ptrs,
-                 const void* tune_rowptr = nullptr, int64_t tune_nnz = 0, const void* tune_tag = nullptr) {
+                 const void* tune_rowptr = nullptr, int64_t tune_nnz = 0, const void* tune_tag = nullptr,
+                 const void* fallback_tag = nullptr) {
   Cfg c;
   const DevInfo d = dev_info();
   if (k == 1) {
     c.G = g1;
     c.KV = 1;
     if (tune_rowptr) {  // autotuned lanes per row (1..32), when the tuner has run
-      const int tg = tuned_g(tune_rowptr, tune_nnz, 1, int(sizeof(T)), 1, tune_tag);
+      int tg = tuned_g(tune_rowptr, tune_nnz, 1, int(sizeof(T)), 1, tune_tag);
+      if (!tg && fallback_tag) tg = tuned_g(tune_rowptr, tune_nnz, 1, int(sizeof(T)), 1, fallback_tag);
       if (tg == 1 || tg == 2 || tg == 4 || tg == 8 || tg == 16 || tg == 32) c.G = tg;
     }
   } else {
@@ -288,6 +303,7 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     c.G = std::max(4, std::min(32, pow2ceil(nch)));
     int tg = 0;
     if (tune_rowptr) tg = tuned_g(tune_rowptr, tune_nnz, k, int(sizeof(T)), c.KV, tune_tag);
+    if (tune_rowptr && !tg && fallback_tag) tg = tuned_g(tune_rowptr, tune_nnz, k, int(sizeof(T)), c.KV, fallback_tag);
     if (const char* fg = std::getenv("AMG_KB_G")) {  // manual override (experiments)
       const int g = atoi(fg);
       const int gl = g >= kWideCode ? g - kWideCode : g >= kLeanCode ? g - kLeanCode : g;
@@ -434,7 +450,7 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
   using V = typename Op::V;
   const V* vals = M.template vals<V>();
   if (M.nnz > 0 && !vals) fail(AMG_ERR_INVALID_ARG, "matrix values missing for this precision");
-  const Cfg c = cfg_k<typename Op::Acc>(M.n_rows, k, M.g1, ptrs, M.rowptr, M.nnz, op_tag<Op>());
+  const Cfg c = cfg_k<typename Op::Acc>(M.n_rows, k, M.g1, ptrs, M.rowptr, M.nnz, op_tag_for(op), op_tag<Op>());
   RedCtx rc{red.partials, red.counter, k};
   if (op.reduces() && !red.partials) fail(AMG_ERR_INVALID_ARG, "reduction scratch missing");
   if (k == 1) {
@@ -497,7 +513,7 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
   if (M.nnz > 0 && !M.template vals<typename Op::V>()) return;
   const int kv = k == 1 ? 1 : pick_kv<T>(k, ptrs);
   if (!tuning_enabled()) return;
-  const void* tag = op_tag<Op>();
+  const void* tag = op_tag_for(op);
   if (tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag)) return;
   const int nch = k / kv;
   const int gmax = std::max(4, std::min(32, pow2ceil(nch)));
