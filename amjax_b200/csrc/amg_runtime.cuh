@@ -502,7 +502,7 @@ bool tuning_enabled();
 // each candidate lanes-per-row G (each with its chunks per lane) and keep the fastest for
 // this (matrix, k, type, op).  Runs outside stream capture, once per key.
 // `before` (optional) runs ahead of every launch, outside the timed region: it restores
-// state an op's finalisation changes (the CG update freezes columns it judges converged,
+// state an op's finalisation changes (the CG update freezes the columns that have converged,
 // and frozen columns skip their writes, which would flatter later candidates).
 template <class Op>
 void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
