@@ -65,11 +65,15 @@ def needs_grad(b, A) -> bool:
 
 class _SolveFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, ml, opts, a_obj, b, a_tensor):
+    def forward(ctx, ml, opts, a_obj, b, a_tensor, x0):
+        """x = x0 + A^-1 b, where b is already shifted to b - A x0 (x0 None: zero)."""
         del a_tensor  # carried only so autograd tracks it
         A0 = _forward_operator(ml, a_obj)
         x = _run(ml, opts, b.detach(), A0)
+        if x0 is not None:
+            x = x + x0
         ctx.ml, ctx.opts, ctx.a_obj = ml, opts, a_obj
+        # dL/dA = -lambda x^T with the FULL solution x (the x0 term comes from b - A x0)
         ctx.save_for_backward(x)
         return x
 
@@ -87,7 +91,7 @@ class _SolveFn(torch.autograd.Function):
             lam2 = lam.reshape(lam.shape[0], -1)
             x2 = x.reshape(x.shape[0], -1)
             grad_a = (-(lam2 @ x2.T)).to(a_obj.dtype).to(a_obj.device)
-        return None, None, None, lam, grad_a
+        return None, None, None, lam, grad_a, None
 
 
 def _forward_operator(ml, a_obj):
@@ -133,7 +137,9 @@ def sampled_outer(pattern: CSRMatrix, lam: torch.Tensor, x: torch.Tensor) -> tor
 
 def solve_with_grad(ml, b, A=None, x0=None, tol=1e-5, maxiter=100, cycle="V", cycles_per_level=1,
                     precision=None, return_info=False, method="solve", atol=0.0):
-    """Differentiable ``solve`` / ``pcg`` (x0 is treated as a constant)."""
+    """Differentiable ``solve`` / ``pcg`` (x0 is treated as a constant).  With x0 the
+    solve runs on b - A x0 and adds x0 back; the gradient with respect to A still uses
+    the full solution, as differentiating b - A x0 through the reference gives."""
     if method == "pcg" and maxiter is None:
         maxiter = 10 * ml.levels[0].A.shape[0]
     opts = dict(tol=tol, atol=atol, maxiter=maxiter, cycle=cycle, cycles_per_level=cycles_per_level,
@@ -150,8 +156,6 @@ def solve_with_grad(ml, b, A=None, x0=None, tol=1e-5, maxiter=100, cycle="V", cy
         A0 = _forward_operator(ml, A)
         Aop = A0 if A0 is not None else ml.levels[0].A
         bt = bt - Aop.matvec(x0t)
-    x = _SolveFn.apply(ml, opts, A, bt, a_tensor)
-    if x0 is not None:
-        x = x + x0t
+    x = _SolveFn.apply(ml, opts, A, bt, a_tensor, x0t if x0 is not None else None)
     info = ml.last_info
     return (x, info) if return_info else x

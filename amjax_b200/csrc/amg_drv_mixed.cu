@@ -1,5 +1,5 @@
 // amg_drv_mixed.cu -- mixed-precision drivers: FP32 cycle inside FP64 refinement / FP64 CG.
-#include "amg_pcg.cuh"
+#include "amg_drivers.cuh"
 
 namespace amg {
 
@@ -43,15 +43,6 @@ void solve_mixed(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
   }
   run_loop(pl, req_key("solve", q), user, prologue, body, [](cudaStream_t) {}, true, q.maxiter + 2);
 }
-
-
-template <class TO, class TC>
-void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
-  Emit pro, bod;
-  pcg_emit<TO, TC>(h, pl, q, user, &pro, &bod);
-  run_loop(pl, req_key("pcg", q), user, pro, bod, [](cudaStream_t) {}, true, q.maxiter + 2);
-}
-
 
 
 template void pcg<double, float>(amg_hierarchy*, Plan*, const Req&, cudaStream_t);

@@ -89,7 +89,9 @@ extern "C" amg_status amg_jacobi_noalloc(const amg_csr* A, int32_t dtype, const 
     check_vec(b, "b");
     check_vec(dinv, "dinv");
     check_vec(out, "out");
-    if (x == out) fail(AMG_ERR_INVALID_ARG, "out may not alias x");
+    // every sweep reads x (first sweep), b and dinv while it writes out
+    if (x == out || b == out || dinv == out) fail(AMG_ERR_INVALID_ARG, "out may not alias x, b or dinv");
+    if (dtype != 0 && dtype != 1) fail(AMG_ERR_INVALID_ARG, "dtype must be 0 (FP64) or 1 (FP32)");
     if (k < 1 || iterations < 0) fail(AMG_ERR_INVALID_ARG, "bad k or iterations");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (iterations == 0) {

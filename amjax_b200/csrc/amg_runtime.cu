@@ -57,6 +57,18 @@ const char* tune_file_path() {
   return (p && p[0]) ? p : nullptr;
 }
 
+// A lanes-per-row code the launchers accept: k == 1: G in {1, 2, 4, 8, 16, 32}; k > 1: a
+// plain code G in {4, 8, 16, 32}, or a lean / wide code (kLeanCode / kWideCode + G) with G
+// in {1, 2, 4, 8, 16, 32}.  A stale or edited tuning-file line with any other value would
+// otherwise reach a launcher that maps it to a layout covering fewer columns than k.
+bool valid_layout_code(int g, int k) {
+  auto lanes = [](int v) { return v == 1 || v == 2 || v == 4 || v == 8 || v == 16 || v == 32; };
+  if (k == 1) return lanes(g);
+  if (g >= kWideCode) return lanes(g - kWideCode);
+  if (g >= kLeanCode) return lanes(g - kLeanCode);
+  return g == 4 || g == 8 || g == 16 || g == 32;
+}
+
 void load_tune_file() {  // g_tune_mu held
   if (g_tune_file_loaded) return;
   g_tune_file_loaded = true;
@@ -68,7 +80,7 @@ void load_tune_file() {  // g_tune_mu held
   long long nnz;
   int k, es, kv, g;
   while (fscanf(f, "%511s %lld %d %d %d %d", name, &nnz, &k, &es, &kv, &g) == 6)
-    g_tune_file[FileKey(name, nnz, k, es, kv)] = g;
+    if (valid_layout_code(g, k)) g_tune_file[FileKey(name, nnz, k, es, kv)] = g;  // others: ignored
   fclose(f);
 }
 }  // namespace

@@ -327,6 +327,11 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
       c.lean = false;
       c.G = std::max(4, std::min(32, pow2ceil(nch)));
     }
+    if ((k / c.KV + c.G - 1) / c.G > kMaxCh) {  // a recorded layout too narrow for this k
+      c.lean = c.wide = false;
+      c.KV = pick_kv<T>(k, ptrs);
+      c.G = std::max(4, std::min(32, pow2ceil(k / c.KV)));
+    }
     const int per = (k / c.KV + c.G - 1) / c.G;
     if (per > kMaxCh)
       fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);

@@ -1,15 +1,23 @@
-"""Smoother set-up and configuration (amjax/relaxation/smoothing.py).
+"""Smoother configuration (the interface of amjax/relaxation/smoothing.py).
 
-Host-side only: a smoother spec (``'jacobi'``, ``('jacobi', {...})``, a list, or
-``None``) becomes one callable per level.  The callables carry their resolved
-parameters (``_amg_spec = (kind, iterations, omega)``) which the native cycle reads;
-calling one directly runs the fused Jacobi kernel.  Errors and flags follow the
-reference: ``ValueError`` for unknown or non-string names (smoothing.py:144-156),
-``NotImplementedError`` for the names the reference lists as not implemented
-(smoothing.py:120-127), ``symmetric_smoothing`` as in smoothing.py:212-228.
+A user writes a smoother as a name (``'jacobi'``), a ``(name, options)`` pair, ``None``
+(no smoothing), or a list of those (one per level, the last repeated downwards).  This
+module turns that into one resolved :class:`SmootherSpec` per level and, from it, the
+level's callable.  The callable carries ``_amg_spec = (kind, iterations, omega)``, the
+resolved numbers the native cycle reads; calling it runs the fused CUDA Jacobi sweep.
+
+Kept identical to the reference because callers and its tests depend on them: the
+exception types and messages (``ValueError`` for unknown or non-string names and bad
+specs, smoothing.py:43-56,130-158; ``NotImplementedError`` for the names listed as not
+implemented, smoothing.py:120-127), the ``symmetric_smoothing`` rule (same name, same
+sweep count, name 'jacobi' or None; smoothing.py:212-228), ``withrho`` dividing omega by
+the estimated spectral radius of D^-1 A once per level, and the per-level
+``_presmoother_spec`` / ``_postsmoother_spec`` records with omega already resolved.
 """
 
 from __future__ import annotations
+
+from dataclasses import dataclass, field
 
 from . import relaxation
 
@@ -26,114 +34,132 @@ _NOT_IMPLEMENTED_SMOOTHERS = {
 }
 
 
-def _unpack_arg(v):
-    """(name, kwargs) of a spec (smoothing.py:36-40)."""
-    if isinstance(v, tuple):
-        return v[0], v[1]
-    return v, {}
+@dataclass(frozen=True)
+class SmootherSpec:
+    """One level's smoother as the user wrote it: ``name`` (a string or None, unchanged)
+    and its keyword options."""
+
+    name: object
+    options: dict = field(default_factory=dict)
+
+    @staticmethod
+    def of(item) -> "SmootherSpec":
+        if isinstance(item, tuple):
+            return SmootherSpec(item[0], item[1])
+        return SmootherSpec(item, {})
+
+    @property
+    def sweeps(self):
+        return self.options.get("iterations", DEFAULT_NITER)
 
 
-def _as_list(v):
-    """smoothing.py:43-49."""
-    if isinstance(v, list):
-        return v
-    if isinstance(v, (str, tuple)) or v is None:
-        return [v]
-    raise ValueError(f"Unrecognized smoother specification: {v!r}")
-
-
-def _expand_to_n(specs, n):
-    """Repeat the last spec until there are n (smoothing.py:52-56)."""
-    if not specs:
+def specs_per_level(spec, n_levels: int) -> list:
+    """The smoother of each of ``n_levels`` levels: a single spec applies to all of them,
+    a list gives level i its i-th entry and the last entry to every level beyond it."""
+    if isinstance(spec, list):
+        items = spec
+    elif spec is None or isinstance(spec, (str, tuple)):
+        items = [spec]
+    else:
+        raise ValueError(f"Unrecognized smoother specification: {spec!r}")
+    if not items:
         raise ValueError("Empty smoother specification.")
-    return (specs + [specs[-1]] * n)[:n]
-
-
-def _bake_kwargs(kw, smoother):
-    """Freeze a withrho-resolved omega into the kwargs (smoothing.py:59-82)."""
-    if not kw.get("withrho", False):
-        return dict(kw)
-    return {**kw, "omega": smoother._omega, "withrho": False}
+    return [SmootherSpec.of(items[min(i, len(items) - 1)]) for i in range(n_levels)]
 
 
 def setup_jacobi(lvl, iterations=DEFAULT_NITER, omega=1.0, withrho=False):
-    """Damped Jacobi on this level (smoothing.py:85-99); withrho divides omega by the
-    power-iteration estimate of rho(D^-1 A), computed once per level."""
-    Dinv = lvl.Dinv
+    """Damped Jacobi on ``lvl`` (smoothing.py:85-99).  ``withrho`` scales omega by
+    1/rho(D^-1 A), the power-iteration estimate, computed once and kept on the level."""
     if withrho:
-        if not hasattr(lvl, "_spectral_radius"):
-            lvl._spectral_radius = relaxation.approximate_spectral_radius(lvl.A, Dinv)
-        omega = omega / lvl._spectral_radius
+        rho = getattr(lvl, "_spectral_radius", None)
+        if rho is None:
+            rho = relaxation.approximate_spectral_radius(lvl.A, lvl.Dinv)
+            lvl._spectral_radius = rho
+        omega = omega / rho
+    dinv = lvl.Dinv
+    sweeps, w = int(iterations), float(omega)
 
-    def smoother(A, x, b):
-        return relaxation.jacobi(A, x, b, Dinv, iterations=iterations, omega=omega)
+    def jacobi_smoother(A, x, b):
+        return relaxation.jacobi(A, x, b, dinv, iterations=sweeps, omega=w)
 
-    smoother.__name__ = "jacobi"
-    smoother._omega = omega
-    smoother._amg_spec = ("jacobi", int(iterations), float(omega))
-    return smoother
+    jacobi_smoother.__name__ = "jacobi"
+    jacobi_smoother._omega = omega
+    jacobi_smoother._amg_spec = ("jacobi", sweeps, w)
+    return jacobi_smoother
 
 
 def setup_none(lvl, **kwargs):
-    """Identity smoother (smoothing.py:102-117)."""
+    """The identity smoother (smoothing.py:102-117): returns x unchanged."""
     del lvl, kwargs
 
-    def smoother(A, x, b):
-        del A, b
+    def identity_smoother(A, x, b):
         return x
 
-    smoother.__name__ = "none"
-    smoother._amg_spec = ("none", 0, 1.0)
-    return smoother
+    identity_smoother.__name__ = "none"
+    identity_smoother._amg_spec = ("none", 0, 1.0)
+    return identity_smoother
 
 
-def _setup_call(fn):
-    """Registry lookup with the reference's error rules (smoothing.py:130-158)."""
-    registry = {"jacobi": setup_jacobi, "none": setup_none}
-    if fn is None:
-        fn = "none"
-    if not isinstance(fn, str):
-        raise ValueError(f"Smoother name must be a string or None, got {fn!r}")
-    if fn in _NOT_IMPLEMENTED_SMOOTHERS:
+_FACTORIES = {"jacobi": setup_jacobi, "none": setup_none}
+
+
+def _factory(name):
+    """The set-up function for ``name`` (None means 'none'), with the reference's errors."""
+    key = "none" if name is None else name
+    if not isinstance(key, str):
+        raise ValueError(f"Smoother name must be a string or None, got {key!r}")
+    if key in _NOT_IMPLEMENTED_SMOOTHERS:
         raise NotImplementedError(
-            f"'{fn}' smoother is not yet implemented in AMJax. Available: {sorted(registry)}")
-    if fn not in registry:
-        raise ValueError(f"Unknown smoother {fn!r}. Available: {sorted(registry)}")
-    return registry[fn]
+            f"'{key}' smoother is not yet implemented in AMJax. Available: {sorted(_FACTORIES)}")
+    try:
+        return _FACTORIES[key]
+    except KeyError:
+        raise ValueError(f"Unknown smoother {key!r}. Available: {sorted(_FACTORIES)}") from None
+
+
+def _resolved_options(spec: SmootherSpec, built) -> dict:
+    """The options with a withrho-scaled omega written in (so a rebuild needs no rho)."""
+    opts = dict(spec.options)
+    if opts.get("withrho", False):
+        opts.update(omega=built._omega, withrho=False)
+    return opts
+
+
+def _build(lvl, spec: SmootherSpec):
+    fn = _factory(spec.name)(lvl, **spec.options)
+    return fn, (spec.name, _resolved_options(spec, fn))
+
+
+def _is_symmetric_pair(pre: SmootherSpec, post: SmootherSpec) -> bool:
+    return pre.name == post.name and pre.sweeps == post.sweeps and pre.name in SYMMETRIC_RELAXATION
 
 
 def change_smoothers(ml, presmoother, postsmoother):
-    """Assign pre/post smoothers on every level but the coarsest
-    (smoothing.py:161-228); sets ``ml.symmetric_smoothing``."""
-    n = len(ml.levels[:-1])
-    if n == 0:
+    """Give every level but the coarsest its pre- and post-smoother (smoothing.py:161-228)
+    and set ``ml.symmetric_smoothing``."""
+    n = len(ml.levels) - 1
+    if n <= 0:
         return
-    pre_specs = _expand_to_n(_as_list(presmoother), n)
-    post_specs = _expand_to_n(_as_list(postsmoother), n)
-    ml.symmetric_smoothing = True
-    for i in range(n):
-        pre_fn, pre_kw = _unpack_arg(pre_specs[i])
-        post_fn, post_kw = _unpack_arg(post_specs[i])
-        lvl = ml.levels[i]
-        lvl.presmoother = _setup_call(pre_fn)(lvl, **pre_kw)
-        lvl.postsmoother = _setup_call(post_fn)(lvl, **post_kw)
-        lvl._presmoother_spec = (pre_fn, _bake_kwargs(pre_kw, lvl.presmoother))
-        lvl._postsmoother_spec = (post_fn, _bake_kwargs(post_kw, lvl.postsmoother))
-        it1 = pre_kw.get("iterations", DEFAULT_NITER)
-        it2 = post_kw.get("iterations", DEFAULT_NITER)
-        if it1 != it2 or pre_fn != post_fn or pre_fn not in SYMMETRIC_RELAXATION:
-            ml.symmetric_smoothing = False
+    pres = specs_per_level(presmoother, n)
+    posts = specs_per_level(postsmoother, n)
+    symmetric = True
+    for lvl, pre, post in zip(ml.levels[:n], pres, posts):
+        lvl.presmoother, lvl._presmoother_spec = _build(lvl, pre)
+        lvl.postsmoother, lvl._postsmoother_spec = _build(lvl, post)
+        symmetric = symmetric and _is_symmetric_pair(pre, post)
+    ml.symmetric_smoothing = symmetric
     if hasattr(ml, "_invalidate"):
         ml._invalidate()
 
 
 def rebuild_smoother(lvl):
-    """Rebuild a level's smoothers from its stored specs (smoothing.py:231-254)."""
-    if getattr(lvl, "_presmoother_spec", None) is None:
-        raise AttributeError("Missing _presmoother_spec on level.")
-    if getattr(lvl, "_postsmoother_spec", None) is None:
-        raise AttributeError("Missing _postsmoother_spec on level.")
-    fn1, kw1 = lvl._presmoother_spec
-    fn2, kw2 = lvl._postsmoother_spec
-    lvl.presmoother = _setup_call(fn1)(lvl, **kw1)
-    lvl.postsmoother = _setup_call(fn2)(lvl, **kw2)
+    """Re-create a level's smoothers from its recorded specs (smoothing.py:231-254)."""
+    recorded = []
+    for attr, label in (("_presmoother_spec", "_presmoother_spec"), ("_postsmoother_spec", "_postsmoother_spec")):
+        rec = getattr(lvl, attr, None)
+        if rec is None:
+            raise AttributeError(f"Missing {label} on level.")
+        recorded.append(rec)
+    (pre_name, pre_opts), (post_name, post_opts) = recorded
+    lvl.presmoother = _factory(pre_name)(lvl, **pre_opts)
+    lvl.postsmoother = _factory(post_name)(lvl, **post_opts)

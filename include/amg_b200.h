@@ -146,7 +146,8 @@ amg_status amg_pcg_batch(amg_hierarchy* const* hs, int32_t nsys, int32_t precisi
                          int32_t* iters_out, double* relres_out, void* stream);
 
 /* Damped Jacobi sweeps on one CSR matrix (amjax/relaxation/relaxation.py:64-98).
- * dtype 0 = FP64 (x, b, dinv, out double), 1 = FP32.  out may not alias x. */
+ * dtype 0 = FP64 (x, b, dinv, out double), 1 = FP32.  out may not alias x, b or dinv
+ * (AMG_ERR_INVALID_ARG). */
 amg_status amg_jacobi(const amg_csr* A, int32_t dtype, const void* x, const void* b,
                       const void* dinv, void* out, int32_t k, int32_t iterations,
                       double omega, void* stream);
