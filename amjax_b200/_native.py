@@ -17,7 +17,7 @@ AMG_OK = 0
 STATUS_NAMES = {0: "AMG_OK", 1: "AMG_ERR_INVALID_ARG", 2: "AMG_ERR_UNSUPPORTED", 3: "AMG_ERR_CUDA",
                 4: "AMG_ERR_TIMEOUT", 5: "AMG_ERR_BAD_MATRIX"}
 CYCLES = {"V": 0, "W": 1, "F": 2}
-PREC_F64, PREC_F32, PREC_MIXED = 0, 1, 2
+PREC_F64, PREC_F32, PREC_MIXED, PREC_MIXED_F64CG = 0, 1, 2, 3
 SMOOTH_NONE, SMOOTH_JACOBI = 0, 1
 COARSE_KINDS = {"pinv": 0, "lu": 1, "qr": 2, "jacobi": 3}
 

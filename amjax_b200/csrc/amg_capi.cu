@@ -4,7 +4,7 @@
 // ======================================================================= C ABI
 using namespace amg;
 
-template <class TO, class TC>
+template <class TO, class TC, bool RU = false>
 static void pcg_batch_impl(amg_hierarchy* const* hs, int nsys, int precision, const void* const* b,
                            void* const* x, const int32_t* k, double tol, double atol, int maxiter,
                            int cycle, int cpl, int32_t* iters_out, double* relres_out, cudaStream_t s) {
@@ -17,12 +17,13 @@ static void pcg_batch_impl(amg_hierarchy* const* hs, int nsys, int precision, co
     BatchSys bs;
     bs.pl = pl;
     bs.gmax = maxiter + 2;
-    pcg_emit<TO, TC>(hs[i], pl, q, s, &bs.pro, &bs.body);
+    if constexpr (RU) pcg_ru_emit<TC>(hs[i], pl, q, s, &bs.pro, &bs.body, &bs.epi);
+    else pcg_emit<TO, TC>(hs[i], pl, q, s, &bs.pro, &bs.body);
     sys.push_back(std::move(bs));
     plans.push_back(pl);
     char buf[48];
     snprintf(buf, sizeof(buf), "/%p:", (void*)hs[i]);
-    key += buf + req_key("pcg", q);
+    key += buf + req_key(RU ? "pcg-ru" : "pcg", q);
   }
   run_batch(sys, key, s);
   size_t off = 0;
@@ -149,7 +150,7 @@ amg_status amg_solve(amg_hierarchy* h, int32_t precision, const void* b, void* x
     Req q{precision, k, cycle, cycles_per_level, maxiter, tol, 0.0, b, x, pa0};
     if (precision == AMG_PREC_F64) solve_plain<double>(h, pl, q, s);
     else if (precision == AMG_PREC_F32) solve_plain<float>(h, pl, q, s);
-    else if (precision == AMG_PREC_MIXED) solve_mixed(h, pl, q, s);
+    else if (is_mixed(precision)) solve_mixed(h, pl, q, s);
     else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
     read_results(pl, s, false, iters_out, relres_out);
   });
@@ -170,7 +171,7 @@ amg_status amg_precondition(amg_hierarchy* h, int32_t precision, const void* b, 
     Plan* pl = get_plan(h, precision, k, s);
     Req q{precision, k, cycle, cycles_per_level, 0, 0.0, 0.0, b, x, nullptr};
     if (precision == AMG_PREC_F64) precondition<double>(h, pl, q, s);
-    else if (precision == AMG_PREC_F32 || precision == AMG_PREC_MIXED) precondition<float>(h, pl, q, s);
+    else if (precision == AMG_PREC_F32 || is_mixed(precision)) precondition<float>(h, pl, q, s);
     else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
   });
 }
@@ -198,7 +199,8 @@ amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, 
     Req q{precision, k, cycle, cycles_per_level, maxiter, tol, atol, b, x, pa0};
     if (precision == AMG_PREC_F64) pcg<double, double>(h, pl, q, s);
     else if (precision == AMG_PREC_F32) pcg<float, float>(h, pl, q, s);
-    else if (precision == AMG_PREC_MIXED) pcg<double, float>(h, pl, q, s);
+    else if (precision == AMG_PREC_MIXED && (!pa0 || pa0->v32)) pcg_ru(h, pl, q, s);
+    else if (is_mixed(precision)) pcg<double, float>(h, pl, q, s);
     else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
     read_results(pl, s, true, iters_out, relres_out);
   });
@@ -306,6 +308,8 @@ amg_status amg_pcg_batch(amg_hierarchy* const* hs, int32_t nsys, int32_t precisi
     else if (precision == AMG_PREC_F32)
       pcg_batch_impl<float, float>(hs, nsys, precision, b, x, k, tol, atol, maxiter, cycle, cycles_per_level, iters_out, relres_out, s);
     else if (precision == AMG_PREC_MIXED)
+      pcg_batch_impl<double, float, true>(hs, nsys, precision, b, x, k, tol, atol, maxiter, cycle, cycles_per_level, iters_out, relres_out, s);
+    else if (precision == AMG_PREC_MIXED_F64CG)
       pcg_batch_impl<double, float>(hs, nsys, precision, b, x, k, tol, atol, maxiter, cycle, cycles_per_level, iters_out, relres_out, s);
     else
       fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);

@@ -609,6 +609,41 @@ struct LoopCtl {
   __device__ __forceinline__ void set_any(int any) const {
     if (!any) *stop = 1;
   }
+
+  // ---- CG with reliable updates (FP32 CG vectors; the FP64 solution and the FP64 true
+  // residual are brought up to date on demand).  State besides the above:
+  double* rmax = nullptr;  // per column: the largest <r, r> since the last true residual
+  int* ru = nullptr;       // ru[0]: a true residual is due; ru[1]: some FP32 increment is unfolded
+  double delta2 = 0.0;     // a true residual is due once <r, r> < delta2 * rmax
+
+  // After the FP32 update of an active column: the column always stays active here (only
+  // the FP64 true residual may retire it); a true residual is requested when the
+  // recursive residual has dropped by delta (the FP32 recurrence has drifted for a while),
+  // when it says the column has converged (confirmed in FP64 before stopping), at maxiter,
+  // or when it is not a number.
+  __device__ __forceinline__ int cg_col_ru(int c, double rr) const {
+    nr[c] = rr;
+    if (!active[c]) return 0;
+    iters[c] += 1;
+    ru[1] = 1;
+    if (rr <= thresh[c] || iters[c] >= maxiter || rr < delta2 * rmax[c] || !(rr == rr)) ru[0] = 1;
+    return 1;
+  }
+  // After the FP64 true residual: the CG rule on the true <r, r> for the columns still
+  // active (frozen columns keep their last values).
+  __device__ __forceinline__ int true_col(int c, double rr) const {
+    if (!active[c]) return 0;
+    nr[c] = rr;
+    rmax[c] = rr;
+    const int a = (rr > thresh[c]) && (iters[c] < maxiter);
+    active[c] = a;
+    return a;
+  }
+  __device__ __forceinline__ void true_all(int any) const {
+    ru[0] = 0;
+    ru[1] = 0;
+    set_any(any);
+  }
 };
 
 // ------------------------------------------------------------------ x sources
@@ -747,7 +782,9 @@ struct OpJacobi {
 
 // r = b - A x (x from an XSource).  RLO: also/instead store a copy in another type.
 // NORM: reduce ||r||^2 per column and apply the standalone loop rule (outer loop of the
-// mixed-precision refinement).  STORE: write r in T.
+// mixed-precision refinement), or with `true_rule` the CG rule of the reliable-update CG
+// (the FP64 true residual).  STORE: write r in T.  `gate` (nullable): the launch returns
+// at once unless *gate is set (the true residual runs only when one is due).
 template <class T, class VT, int XS, bool STORE, class TLO, bool NORM>
 struct OpResid {
   static constexpr bool kPrepared = false;
@@ -762,8 +799,10 @@ struct OpResid {
   int ld;
   const int* stop;
   LoopCtl ctl;
+  const int* gate = nullptr;
+  bool true_rule = false;
 
-  __device__ __forceinline__ bool stopped() const { return stop && *stop; }
+  __device__ __forceinline__ bool stopped() const { return (stop && *stop) || (gate && !*gate); }
   __device__ __forceinline__ T x1(int j) const { return xs.get1(j); }
   template <int KV>
   __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const { xs.template getk<KV>(j, c0, v); }
@@ -795,11 +834,14 @@ struct OpResid {
     }
   }
   __device__ __forceinline__ int finalize_col(int c, double s) const {
-    if constexpr (NORM) return ctl.standalone_col(c, s);
+    if constexpr (NORM) return true_rule ? ctl.true_col(c, s) : ctl.standalone_col(c, s);
     return 1;
   }
   __device__ __forceinline__ void finalize_all(int any) const {
-    if constexpr (NORM) ctl.set_any(any);
+    if constexpr (NORM) {
+      if (true_rule) ctl.true_all(any);
+      else ctl.set_any(any);
+    }
   }
 };
 
@@ -994,11 +1036,48 @@ struct OpCgUpdA {
       st_vec<TLO, KV>(r_lo + o, rl);
     }
   }
-  __device__ __forceinline__ int finalize_col(int c, double s) const { return ctl.cg_col(c, s); }
-  __device__ __forceinline__ void finalize_all(int any) const { ctl.set_any(any); }
+  // reliable: the CG of the reliable-update form (x and r are the FP32 increment and
+  // residual; retiring columns is left to the FP64 true residual)
+  bool reliable = false;
+  __device__ __forceinline__ int finalize_col(int c, double s) const {
+    return reliable ? ctl.cg_col_ru(c, s) : ctl.cg_col(c, s);
+  }
+  __device__ __forceinline__ void finalize_all(int any) const {
+    if (!reliable) ctl.set_any(any);
+  }
 };
 
 // ------------------------------------------------------------------ elementwise ops
+// Reliable-update fold: x += xs (FP64 solution += FP32 increment), xs = 0, every column
+// (retired columns hold a zero increment).  Runs only when *gate is set.
+template <class T, class TS>
+struct OpFold {
+  static constexpr bool kReduce = false;
+  __host__ __device__ __forceinline__ bool reduces() const { return kReduce; }
+  T* x;
+  TS* xs;
+  int ld;
+  const int* gate;
+  __device__ __forceinline__ bool stopped() const { return !*gate; }
+  template <int KV>
+  __device__ __forceinline__ void elem(int i, int c0, double (&)[KV]) const {
+    const size_t o = voff(i, ld, c0);
+    T xv[KV];
+    TS sv[KV], zero[KV];
+    ld_vec<T, KV>(x + o, xv);
+    ld_vec<TS, KV>(xs + o, sv);
+#pragma unroll
+    for (int v = 0; v < KV; ++v) {
+      xv[v] += static_cast<T>(sv[v]);
+      zero[v] = TS(0);
+    }
+    st_vec<T, KV>(x + o, xv);
+    st_vec<TS, KV>(xs + o, zero);
+  }
+  __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
+  __device__ __forceinline__ void finalize_all(int) const {}
+};
+
 // CG update: for active columns x += alpha p, r -= alpha q; copy r into the cycle's
 // type (r_lo, nullable); reduce <r, r> and apply the CG loop rule.
 template <class T, class TLO>
@@ -1127,6 +1206,8 @@ struct OpSetup {
   int* gcount;
   double tol, atol;
   int maxiter;
+  double* rmax = nullptr;  // reliable-update CG: rmax = <b, b>, no true residual due
+  int* ru = nullptr;
   __device__ __forceinline__ bool stopped() const { return false; }
   template <int KV>
   __device__ __forceinline__ void elem(int i, int c0, double (&red)[KV]) const {
@@ -1163,6 +1244,7 @@ struct OpSetup {
       const double t = fmax(tol * tol * s, atol * atol);
       thresh[c] = t;
       nr[c] = s;
+      if (rmax) rmax[c] = s;
       const int a = (s > t) && (maxiter > 0);
       active[c] = a;
       return a;
@@ -1170,6 +1252,7 @@ struct OpSetup {
   }
   __device__ __forceinline__ void finalize_all(int any) const {
     if (gcount) *gcount = 0;
+    if (ru) ru[0] = ru[1] = 0;
     *stop = (MODE == 0) ? 0 : (any ? 0 : 1);
   }
 };

@@ -202,9 +202,9 @@ Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s) {
   pl->r_out = pl->alloc(n0 * osize);
   pl->p_out = pl->alloc(n0 * osize);
   pl->q_out = pl->alloc(n0 * osize);
-  pl->dscal = static_cast<double*>(pl->alloc(sizeof(double) * 6 * k));
-  pl->iscal = static_cast<int*>(pl->alloc(sizeof(int) * (2 * k + 2)));
-  CK(cudaMemset(pl->iscal, 0, sizeof(int) * (2 * k + 2)));
+  pl->dscal = static_cast<double*>(pl->alloc(sizeof(double) * 7 * k));
+  pl->iscal = static_cast<int*>(pl->alloc(sizeof(int) * (2 * k + 4)));
+  CK(cudaMemset(pl->iscal, 0, sizeof(int) * (2 * k + 4)));
   pl->partials = static_cast<double*>(
       pl->alloc(sizeof(double) * size_t(dev_info().max_ctas + kRedGroups) * k));
   pl->counter = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * (1 + kRedGroups)));
@@ -429,6 +429,7 @@ void run_batch(const std::vector<BatchSys>& systems, const std::string& key, cud
         sy.body(c2);
         launch(loop_guard_kernel, 1, 32, 0, c2, stp, gc, gmax, hc);
       });
+      if (sy.epi) capture(g, &cn, 1, sy.epi);
     }
     CK(cudaGraphInstantiate(&e->exec, g, 0));
     g_batch_graphs.emplace_front(key, std::move(e));
@@ -461,8 +462,23 @@ LoopCtl make_ctl(Plan* pl, int maxiter) {
   c.iters = pl->iters();
   c.stop = pl->stop();
   c.maxiter = maxiter;
+  c.rmax = pl->rmax();
+  c.ru = pl->ru();
+  c.delta2 = ru_delta2();
   return c;
 }
+
+double ru_delta2() {
+  static const double d2 = [] {
+    const char* e = std::getenv("AMG_RU_DELTA");
+    double d = e ? atof(e) : 1e-2;
+    if (!(d > 0.0 && d < 1.0)) d = 1e-2;
+    return d * d;
+  }();
+  return d2;
+}
+
+bool is_mixed(int prec) { return prec == AMG_PREC_MIXED || prec == AMG_PREC_MIXED_F64CG; }
 
 Red red_of(Plan* pl) { return Red{pl->partials, pl->counter}; }
 
@@ -493,7 +509,7 @@ void check_prec_data(amg_hierarchy* h, int prec, const Csr* A0) {
       fail(AMG_ERR_INVALID_ARG, "level %d lacks %s matrix values", l, need64 ? "FP64" : "FP32");
     if (need64 ? !lv.dinv64 : !lv.dinv32) fail(AMG_ERR_INVALID_ARG, "level %d lacks dinv", l);
   }
-  if (prec == AMG_PREC_MIXED) {
+  if (is_mixed(prec)) {
     const Csr& A = A0 ? *A0 : h->levels[0].A;
     if (!A.v64) fail(AMG_ERR_INVALID_ARG, "MIXED needs FP64 values of the level-0 operator");
   }

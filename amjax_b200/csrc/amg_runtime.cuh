@@ -171,8 +171,8 @@ struct Plan {
   void* p_out = nullptr;              // CG direction buffers (outer type): p_out and q_out
   void* q_out = nullptr;              //   alternate as old / new direction per CG step
   void* r_lo = nullptr;               // cycle-type copy of r (MIXED)
-  double* dscal = nullptr;            // per-column doubles: thresh, nr, normb, gamma, alpha, beta
-  int* iscal = nullptr;               // per-column ints: active, iters; then stop, gcount
+  double* dscal = nullptr;            // per-column doubles: thresh, nr, normb, gamma, alpha, beta, rmax
+  int* iscal = nullptr;               // per-column ints: active, iters; then stop, gcount, ru[2]
   double* partials = nullptr;
   unsigned* counter = nullptr;
   int* h_stop = nullptr;              // pinned host mirror of the stop flag (host-loop mode)
@@ -186,10 +186,12 @@ struct Plan {
   double* gamma() { return dscal + 3 * k; }
   double* alpha() { return dscal + 4 * k; }
   double* beta() { return dscal + 5 * k; }
+  double* rmax() { return dscal + 6 * k; }
   int* active() { return iscal; }
   int* iters() { return iscal + k; }
   int* stop() { return iscal + 2 * k; }
   int* gcount() { return iscal + 2 * k + 1; }
+  int* ru() { return iscal + 2 * k + 2; }  // [0] true residual due, [1] FP32 increment unfolded
 
   void* alloc(size_t bytes) {
     void* p = nullptr;
@@ -977,11 +979,18 @@ void solve_mixed(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 template <class TO, class TC> void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 template <class TO, class TC>
 void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit* pro, Emit* bod);
+template <class TC>
+void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit* pro, Emit* bod, Emit* epi);
+void pcg_ru(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
+// Threshold of the reliable-update CG: a true residual is due once the FP32 residual norm
+// has dropped by this factor since the last one (AMG_RU_DELTA, default 1e-2); squared.
+double ru_delta2();
+bool is_mixed(int prec);
 
 // One system of a batch: its plan and its emitters (prologue, loop body).
 struct BatchSys {
   Plan* pl;
-  Emit pro, body;
+  Emit pro, body, epi;  // epi: nullable, after the loop
   int gmax;
 };
 // Capture (once per key) and launch one graph holding every system's loop as an independent

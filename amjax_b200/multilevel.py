@@ -7,8 +7,11 @@ deprecated alias (:730-743).  The hierarchy's CSR arrays are uploaded once into 
 CUDA tensors; ``solve`` / ``pcg`` / the preconditioner each run as one CUDA-graph
 launch of the library's fused kernels (``libamg_b200.so``).  There is no CPU path.
 
-Extensions over the reference, all optional: ``precision`` ('f64' | 'f32' | 'mixed':
-FP32 cycle inside an FP64 refinement / CG loop), right-hand sides stored ``[N, k]`` (k
+Extensions over the reference, all optional: ``precision`` ('f64' | 'f32' | 'mixed' |
+'mixed-f64cg'; 'mixed': FP32 cycle inside FP64 refinement for ``solve``, and for ``pcg``
+an FP32 CG whose FP64 solution and FP64 true residual are refreshed whenever the FP32
+residual has dropped by a fixed factor and before a column stops; 'mixed-f64cg': the FP32
+cycle inside an FP64 CG), right-hand sides stored ``[N, k]`` (k
 columns solved at once, each freezing when converged as ``jax.vmap`` over the solve
 does), ``pcg`` (the fused equivalent of ``jax.scipy.sparse.linalg.cg(A, b,
 M=ml.aspreconditioner())``), ``return_info`` (iterations and final relative residual
@@ -32,7 +35,8 @@ from .relaxation import smoothing
 
 __all__ = ["MultilevelSolver", "multilevel_solver", "coarse_grid_solver", "_NOT_IMPLEMENTED_SOLVERS"]
 
-_PRECISIONS = {"f64": N.PREC_F64, "f32": N.PREC_F32, "mixed": N.PREC_MIXED}
+_PRECISIONS = {"f64": N.PREC_F64, "f32": N.PREC_F32, "mixed": N.PREC_MIXED,
+               "mixed-f64cg": N.PREC_MIXED_F64CG}
 
 
 class _Level:

@@ -43,10 +43,22 @@ typedef enum { AMG_CYCLE_V = 0, AMG_CYCLE_W = 1, AMG_CYCLE_F = 2 } amg_cycle;
  *  F64:   every vector, value and accumulation in FP64.
  *  F32:   FP32 hierarchy end to end (the reference's dtype=float32 mode); sums that
  *         decide convergence are accumulated in FP64.
- *  MIXED: the cycle runs on FP32 values and vectors with FP32 accumulation; the outer
- *         loop (residual b - A x, refinement update, PCG dots/step lengths and the
- *         convergence norm) runs in FP64 on FP64 values. */
-typedef enum { AMG_PREC_F64 = 0, AMG_PREC_F32 = 1, AMG_PREC_MIXED = 2 } amg_precision;
+ *  MIXED: the cycle runs on FP32 values and vectors with FP32 accumulation.  Standalone
+ *         solve: FP64 iterative refinement around the FP32 cycle (residual b - A x, update
+ *         and convergence norm in FP64 on FP64 values).  PCG: CG with reliable updates:
+ *         the CG vectors are FP32 (dot products and step lengths FP64); the FP64 solution
+ *         and the FP64 true residual b - A x are brought up to date whenever the FP32
+ *         residual has dropped by a fixed factor (AMG_RU_DELTA, default 1e-2) and before
+ *         any column stops, so the stop rule is checked on the FP64 residual.  (With an
+ *         A0 that has no FP32 values, PCG falls back to MIXED_F64CG.)
+ *  MIXED_F64CG: as MIXED, except that PCG keeps its vectors in FP64 around the FP32
+ *         cycle (FP64 CG preconditioned by the FP32 cycle). */
+typedef enum {
+  AMG_PREC_F64 = 0,
+  AMG_PREC_F32 = 1,
+  AMG_PREC_MIXED = 2,
+  AMG_PREC_MIXED_F64CG = 3
+} amg_precision;
 
 typedef enum { AMG_SMOOTH_NONE = 0, AMG_SMOOTH_JACOBI = 1 } amg_smoother_kind;
 
@@ -126,9 +138,9 @@ amg_status amg_precondition(amg_hierarchy* h, int32_t precision, const void* b, 
 
 /* Preconditioned CG with M = one cycle (jax.scipy.sparse.linalg.cg(A, b, M=ml.
  * aspreconditioner()) as the reference's benchmark calls it, benchmarks/benchmark.ipynb
- * cell 7; stopping rule <r,r> <= max(tol^2 <b,b>, atol^2)).  b, x FP64 ([n0,k]) for F64
- * and MIXED (FP32 preconditioner inside an FP64 CG), FP32 for F32.  A0 as in amg_solve
- * (used for the CG operator; the preconditioner keeps the hierarchy's level 0). */
+ * cell 7; stopping rule <r,r> <= max(tol^2 <b,b>, atol^2)).  b, x FP64 ([n0,k]) for F64,
+ * MIXED and MIXED_F64CG, FP32 for F32.  A0 as in amg_solve (used for the CG operator;
+ * the preconditioner keeps the hierarchy's level 0). */
 amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, int32_t k,
                    double tol, double atol, int32_t maxiter, int32_t cycle,
                    int32_t cycles_per_level, const amg_csr* A0, int32_t* iters_out,
