@@ -121,6 +121,16 @@ amg_status amg_hierarchy_create(const amg_level_desc* levels, int32_t n_levels,
     if (c.n != h->levels.back().A.n_rows)
       fail(AMG_ERR_INVALID_ARG, "coarse n=%d does not match the coarsest level (%d)", c.n, h->levels.back().A.n_rows);
     if (c.kind == AMG_COARSE_LU && !c.perm) fail(AMG_ERR_INVALID_ARG, "LU coarse solver needs perm");
+    // structure of every operator on the device (the arrays may still be filling on another
+    // stream: wait for the device first)
+    CK(cudaDeviceSynchronize());
+    for (int l = 0; l < n_levels; ++l) {
+      validate_csr(levels[l].A, "A", l, nullptr, false);
+      if (l < n_levels - 1) {
+        validate_csr(levels[l].P, "P", l, nullptr, false);
+        validate_csr(levels[l].R, "R", l, nullptr, false);
+      }
+    }
     h->coarse = c;
     *out = h.release();
   });
@@ -143,11 +153,12 @@ amg_status amg_solve(amg_hierarchy* h, int32_t precision, const void* b, void* x
     std::lock_guard<std::mutex> lk(h->mu);
     Csr a0;
     const Csr* pa0 = nullptr;
-    if (A0) { a0 = override_csr(h, A0); pa0 = &a0; }
-    check_prec_data(h, precision, pa0);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (A0) { a0 = override_csr(h, A0, s); pa0 = &a0; }
+    check_prec_data(h, precision, pa0);
     Plan* pl = get_plan(h, precision, k, s);
     Req q{precision, k, cycle, cycles_per_level, maxiter, tol, 0.0, b, x, pa0};
+    q.program = true;
     if (precision == AMG_PREC_F64) solve_plain<double>(h, pl, q, s);
     else if (precision == AMG_PREC_F32) solve_plain<float>(h, pl, q, s);
     else if (is_mixed(precision)) solve_mixed(h, pl, q, s);
@@ -190,13 +201,14 @@ amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, 
     std::lock_guard<std::mutex> lk(h->mu);
     Csr a0;
     const Csr* pa0 = nullptr;
-    if (A0) { a0 = override_csr(h, A0); pa0 = &a0; }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (A0) { a0 = override_csr(h, A0, s); pa0 = &a0; }
     check_prec_data(h, precision, nullptr);
     if (pa0 && (precision == AMG_PREC_F32 ? !pa0->v32 : !pa0->v64))
       fail(AMG_ERR_INVALID_ARG, "A0 lacks values for this precision");
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     Plan* pl = get_plan(h, precision, k, s);
     Req q{precision, k, cycle, cycles_per_level, maxiter, tol, atol, b, x, pa0};
+    q.program = true;
     if (precision == AMG_PREC_F64) pcg<double, double>(h, pl, q, s);
     else if (precision == AMG_PREC_F32) pcg<float, float>(h, pl, q, s);
     else if (precision == AMG_PREC_MIXED && (!pa0 || pa0->v32)) pcg_ru(h, pl, q, s);
@@ -211,7 +223,7 @@ amg_status amg_jacobi(const amg_csr* A, int32_t dtype, const void* x, const void
                       void* stream) {
   return guarded([&] {
     if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
-    check_csr(*A, "A", 0);
+    validate_csr(*A, "A", 0, static_cast<cudaStream_t>(stream), true);
     check_vec(x, "x"); check_vec(b, "b"); check_vec(dinv, "dinv"); check_vec(out, "out");
     // every sweep reads x (first sweep), b and dinv while it writes out
     if (x == out || b == out || dinv == out) fail(AMG_ERR_INVALID_ARG, "out may not alias x, b or dinv");
@@ -232,7 +244,7 @@ amg_status amg_jacobi(const amg_csr* A, int32_t dtype, const void* x, const void
 amg_status amg_spmv(const amg_csr* A, int32_t dtype, const void* x, void* y, int32_t k, void* stream) {
   return guarded([&] {
     if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
-    check_csr(*A, "A", 0);
+    validate_csr(*A, "A", 0, static_cast<cudaStream_t>(stream), true);
     check_vec(x, "x"); check_vec(y, "y");
     if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -256,7 +268,7 @@ amg_status amg_spmv(const amg_csr* A, int32_t dtype, const void* x, void* y, int
 amg_status amg_inverse_diagonal(const amg_csr* A, int32_t dtype, void* dinv, void* stream) {
   return guarded([&] {
     if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
-    check_csr(*A, "A", 0);
+    validate_csr(*A, "A", 0, static_cast<cudaStream_t>(stream), true);
     check_vec(dinv, "dinv");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int grid = std::max(1, std::min((A->n_rows + 255) / 256, dev_info().max_ctas));
@@ -271,7 +283,7 @@ amg_status amg_sampled_outer(const amg_csr* A, const double* lam, const double* 
                              double* grad, void* stream) {
   return guarded([&] {
     if (!A) fail(AMG_ERR_INVALID_ARG, "null matrix");
-    check_csr(*A, "A", 0);
+    validate_csr(*A, "A", 0, static_cast<cudaStream_t>(stream), true);
     check_vec(lam, "lam"); check_vec(x, "x"); check_vec(grad, "grad");
     if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -320,7 +332,7 @@ int64_t amg_kernel_launch_count(void) {
   if (cudaDeviceSynchronize() != cudaSuccess) return -1;
   unsigned long long mine = 0;
   if (cudaMemcpyFromSymbol(&mine, g_kernel_count, sizeof(mine)) != cudaSuccess) return -1;
-  return int64_t(mine + count_f64() + count_f32() + count_mixed() + count_runtime());
+  return int64_t(mine + count_f64() + count_f32() + count_mixed() + count_runtime() + count_program());
 }
 
 const char* amg_last_error(void) { return t_err.c_str(); }

@@ -23,6 +23,7 @@ void solve_plain(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     cy.h = h; cy.pl = pl; cy.s = cs; cy.k = q.k; cy.stop = pl->stop(); cy.A0 = A0;
     cy.b0 = b; cy.x0 = x; cy.fine_norm = true; cy.ctl = make_ctl(pl, q.maxiter);
     cy.fine_mask = q.k > 1; cy.red = red_of(pl);
+    cy.tail_from = tail_level<T>(h, q.k, q.program);
     cy.visit(0, false, ct, q.cpl);
   };
   autotune_cycle<T>(h, pl, q.k, A0, user);

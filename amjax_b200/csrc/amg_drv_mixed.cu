@@ -29,6 +29,7 @@ void solve_mixed(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
     Cycle<float> cy{};
     cy.h = h; cy.pl = pl; cy.s = cs; cy.k = q.k; cy.stop = pl->stop(); cy.A0 = A0;
     cy.b0 = r32; cy.x0 = e32; cy.red = red_of(pl);
+    cy.tail_from = tail_level<float>(h, q.k, q.program);
     cy.visit(0, true, ct, q.cpl);
     OpRefine<double, float> up{x, e32, pl->active(), q.k, pl->stop()};
     run_elem<float>(n0, up, q.k, red_of(pl), cs, {x, e32});

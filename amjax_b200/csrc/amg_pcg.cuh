@@ -29,11 +29,13 @@ void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit*
   const Csr* A0 = q.A0 ? q.A0 : &h->levels[0].A;
   const int k = q.k, cpl = q.cpl, maxiter = q.maxiter;
   const double tol = q.tol, atol = q.atol;
+  const int tail = tail_level<TC>(h, k, q.program);
   auto cycle = [=](cudaStream_t cs) {
     Cycle<TC> cy{};
     cy.h = h; cy.pl = pl; cy.s = cs; cy.k = k; cy.stop = pl->stop(); cy.A0 = nullptr;
     cy.b0 = rc; cy.x0 = z; cy.fine_dot = r; cy.dot_is_f64 = sizeof(TO) == 8;
     cy.red = red_of(pl);
+    cy.tail_from = tail;
     cy.visit(0, true, ct, cpl);
   };
   auto step = [=](cudaStream_t cs, TO* p_old, TO* p_new) {
@@ -122,11 +124,13 @@ void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Em
   const int k = q.k, cpl = q.cpl, maxiter = q.maxiter;
   const double tol = q.tol, atol = q.atol;
   const LoopCtl ctl = make_ctl(pl, maxiter);
+  const int tail = tail_level<TC>(h, k, q.program);
   auto cycle = [=](cudaStream_t cs) {
     Cycle<TC> cy{};
     cy.h = h; cy.pl = pl; cy.s = cs; cy.k = k; cy.stop = pl->stop(); cy.A0 = nullptr;
     cy.b0 = rs; cy.x0 = z; cy.fine_dot = rs; cy.dot_is_f64 = false;
     cy.red = red_of(pl);
+    cy.tail_from = tail;
     cy.visit(0, true, ct, cpl);
   };
   auto true_residual = [=](cudaStream_t cs) {

@@ -151,6 +151,75 @@ void check_csr(const amg_csr& c, const char* what, int lvl) {
     fail(AMG_ERR_INVALID_ARG, "level %d %s: no values", lvl, what);
 }
 
+// ------------------------------------------------------------------ CSR structure check
+// Status of the last structure check: [0] error bits, [1] the smallest offending row (bits
+// 1, 2, 4) or nonzero (bit 8).  One check runs at a time (g_check_mu).
+static __device__ int g_csr_status[2];
+
+enum : int { kBadRow0 = 1, kBadOrder = 2, kBadEnd = 4, kBadCol = 8 };
+
+// Reads rowptr[0 .. n_rows] and col[0 .. nnz), the extents the descriptor declares.
+__global__ void csr_check_kernel(const int* __restrict__ rowptr, const int* __restrict__ col, int n_rows,
+                                 int n_cols, long long nnz) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  for (long long i = tid; i < n_rows; i += nth) {
+    const int a = rowptr[i], b = rowptr[i + 1];
+    int bad = 0;
+    if (i == 0 && a != 0) bad |= kBadRow0;
+    if (b < a) bad |= kBadOrder;
+    if (i == n_rows - 1 && (long long)b != nnz) bad |= kBadEnd;
+    if (bad) {
+      atomicOr(&g_csr_status[0], bad);
+      atomicMin(&g_csr_status[1], int(i));
+    }
+  }
+  for (long long e = tid; e < nnz; e += nth) {
+    const int c = col[e];
+    if (c < 0 || c >= n_cols) {
+      atomicOr(&g_csr_status[0], kBadCol);
+      atomicMin(&g_csr_status[1], int(e));
+    }
+  }
+}
+
+namespace {
+std::mutex g_check_mu;
+// Structures already checked, by (rowptr, col, n_rows, n_cols, nnz): the stand-alone kernels
+// check a matrix the first time they see it, not on every call.
+std::map<std::tuple<const void*, const void*, int, int, int64_t>, bool> g_checked;
+}  // namespace
+
+void validate_csr(const amg_csr& c, const char* what, int lvl, cudaStream_t s, bool once) {
+  check_csr(c, what, lvl);
+  if (c.n_rows == 0) return;
+  std::lock_guard<std::mutex> lk(g_check_mu);
+  const auto key = std::make_tuple((const void*)c.rowptr, (const void*)c.col, c.n_rows, c.n_cols, c.nnz);
+  if (once && g_checked.count(key)) return;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone) return;  // a capture cannot wait for the verdict
+  const int init[2] = {0, INT32_MAX};
+  CK(cudaMemcpyToSymbolAsync(g_csr_status, init, sizeof(init), 0, cudaMemcpyHostToDevice, s));
+  const long long work = std::max<long long>(c.n_rows, c.nnz);
+  const int grid = int(std::max<long long>(1, std::min<long long>((work + 255) / 256, dev_info().max_ctas)));
+  csr_check_kernel<<<grid, 256, 0, s>>>(c.rowptr, c.col, c.n_rows, c.n_cols, (long long)c.nnz);
+  CK_LAUNCH();
+  int st[2] = {0, 0};
+  CK(cudaMemcpyFromSymbolAsync(st, g_csr_status, sizeof(st), 0, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (st[0] & kBadRow0) fail(AMG_ERR_BAD_MATRIX, "level %d %s: rowptr[0] is not 0", lvl, what);
+  if (st[0] & kBadOrder)
+    fail(AMG_ERR_BAD_MATRIX, "level %d %s: rowptr decreases (first at row %d)", lvl, what, st[1]);
+  if (st[0] & kBadEnd)
+    fail(AMG_ERR_BAD_MATRIX, "level %d %s: rowptr[n_rows] differs from nnz = %lld", lvl, what, (long long)c.nnz);
+  if (st[0] & kBadCol)
+    fail(AMG_ERR_BAD_MATRIX, "level %d %s: column index out of [0, %d) (first at nonzero %d)", lvl, what,
+         c.n_cols, st[1]);
+  if (g_checked.size() > 4096) g_checked.clear();
+  g_checked[key] = true;
+}
+
 // Loop guard: ends each body of the device while-loop.  Sets the loop condition from
 // the stop flag and a hard trip bound, so the loop always terminates.
 __global__ void loop_guard_kernel(int* stop, int* gcount, int gmax, cudaGraphConditionalHandle h) {
@@ -210,6 +279,8 @@ Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s) {
   pl->counter = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * (1 + kRedGroups)));
   CK(cudaMemset(pl->counter, 0, sizeof(unsigned) * (1 + kRedGroups)));
   CK(cudaHostAlloc(reinterpret_cast<void**>(&pl->h_stop), sizeof(int), cudaHostAllocDefault));
+  pl->bar = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * 4));
+  CK(cudaMemset(pl->bar, 0, sizeof(unsigned) * 4));
   Plan* raw = pl.get();
   h->plans[key] = std::move(pl);
   return raw;
@@ -281,6 +352,7 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
                      const Emit& body, const Emit& epilogue, bool has_loop, int gmax) {
   const ExecMode mode = exec_mode();
   if (mode == EXEC_EAGER) {
+    CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * 3, user));
     prologue(user);
     if (has_loop) {
       for (int trip = 0;; ++trip) {
@@ -359,6 +431,8 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
     while (pl->graphs.size() > 8) pl->graphs.pop_back();
     ge = pl->graphs.front().second.get();
   }
+  if (pl->used_program)  // barrier count, generation and status start at 0
+    CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * 3, user));
   if (!ge->host_loop) {
     CK(cudaGraphLaunch(ge->exec, user));
   } else {
@@ -440,6 +514,16 @@ void run_batch(const std::vector<BatchSys>& systems, const std::string& key, cud
 }
 
 void read_results(Plan* pl, cudaStream_t s, bool cg, int32_t* iters_out, double* relres_out) {
+  if (pl->used_program) {  // a persistent program whose barrier wait ran out gave up
+    unsigned st = 0;
+    CK(cudaMemcpyAsync(&st, pl->bar + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (st) {
+      CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * 3, s));
+      fail(AMG_ERR_TIMEOUT, "a grid barrier of the persistent coarse-level kernel ran out of time "
+                            "(AMG_SPIN_LIMIT); the result is not valid");
+    }
+  }
   if (!iters_out && !relres_out) return;
   const int k = pl->k;
   std::vector<int> it(k);
@@ -521,8 +605,8 @@ void check_prec_data(amg_hierarchy* h, int prec, const Csr* A0) {
     fail(AMG_ERR_INVALID_ARG, "coarse QR factor R missing for this precision");
 }
 
-Csr override_csr(amg_hierarchy* h, const amg_csr* A0) {
-  check_csr(*A0, "A0", 0);
+Csr override_csr(amg_hierarchy* h, const amg_csr* A0, cudaStream_t s) {
+  validate_csr(*A0, "A0", 0, s, false);
   const Csr& A = h->levels[0].A;
   if (A0->n_rows != A.n_rows || A0->n_cols != A.n_cols)
     fail(AMG_ERR_INVALID_ARG, "A0 shape %dx%d does not match level 0 (%dx%d)", A0->n_rows, A0->n_cols,

@@ -28,6 +28,7 @@
 
 #include "../../include/amg_b200.h"
 #include "amg_device.cuh"
+#include "amg_program.cuh"
 
 namespace amg {
 
@@ -104,6 +105,11 @@ struct Csr {
 };
 
 void check_csr(const amg_csr& c, const char* what, int lvl);
+// check_csr plus a device pass over the structure on stream s (row pointers start at 0, never
+// decrease and end at nnz; every column in [0, n_cols)), waited for: AMG_ERR_BAD_MATRIX
+// otherwise.  once: skip a structure already checked (same pointers and sizes).  Skipped
+// while s is being captured into a graph.
+void validate_csr(const amg_csr& c, const char* what, int lvl, cudaStream_t s, bool once);
 
 // ------------------------------------------------------------------ hierarchy
 struct Smooth {
@@ -176,6 +182,8 @@ struct Plan {
   double* partials = nullptr;
   unsigned* counter = nullptr;
   int* h_stop = nullptr;              // pinned host mirror of the stop flag (host-loop mode)
+  unsigned* bar = nullptr;            // persistent-program barrier: count, generation, status
+  bool used_program = false;          // some captured solve of this plan runs a program
   std::vector<void*> allocs;
   std::list<std::pair<std::string, std::unique_ptr<GraphEntry>>> graphs;  // LRU
   int64_t nodes_outside = 0, nodes_body = 0;
@@ -703,6 +711,42 @@ struct Cycle {
   const void* fine_dot = nullptr;  // CG: fuse <r, z> into the last level-0 sweep (outer type)
   bool dot_is_f64 = true;
   Red red;
+  int tail_from = -1;                 // levels >= this run as one persistent program (-1: none)
+  std::vector<PStep>* rec = nullptr;  // recording a program: steps are appended, not launched
+
+  template <class Op>
+  void record(const Op& op, int kind, const Csr& M, const void* x, const void* b, const void* dinv,
+              const void* base, void* out, double omega, std::initializer_list<const void*> ptrs) {
+    PStep st{};
+    st.kind = kind;
+    st.n_rows = M.n_rows;
+    st.rowptr = M.rowptr;
+    st.col = M.col;
+    st.val = M.template vals<T>();
+    st.x = x; st.b = b; st.dinv = dinv; st.base = base; st.out = out; st.omega = omega;
+    st.barrier = 1;
+    if (k == 1) {  // the launched kernel's lanes per row (its shuffle order)
+      st.g = cfg_k<T>(M.n_rows, 1, M.g1, ptrs, M.rowptr, M.nnz, op_tag_for(op), op_tag<Op>()).G;
+      st.kv = 1;
+    } else {
+      const int kv16 = 16 / int(sizeof(T));
+      st.kv = (k % kv16 == 0) ? kv16 : 1;
+      st.g = pow2ceil(k / st.kv);
+    }
+    rec->push_back(st);
+  }
+
+  // Run the recorded steps: one cooperative launch per kMaxSteps steps.
+  void emit_program(const std::vector<PStep>& steps) {
+    const GridBar gb{pl->bar, pl->bar + 1, reinterpret_cast<int*>(pl->bar + 2), spin_limit()};
+    for (size_t i0 = 0; i0 < steps.size(); i0 += kMaxSteps) {
+      Program p{};
+      p.nsteps = int(std::min<size_t>(kMaxSteps, steps.size() - i0));
+      for (int j = 0; j < p.nsteps; ++j) p.steps[j] = steps[i0 + size_t(j)];
+      launch_program(p, sizeof(T) == 8, k, stop, gb, s);
+    }
+    pl->used_program = true;
+  }
 
   int L() const { return int(h->levels.size()); }
   const Csr& Aof(int l) const { return (l == 0 && A0) ? *A0 : h->levels[l].A; }
@@ -721,6 +765,13 @@ struct Cycle {
   template <int XS>
   void sweep_x(int l, const T* in, T omega, T* out, bool norm, bool mask, bool dot) {
     const Level& lv = h->levels[l];
+    if (rec) {
+      if (norm || mask || dot) fail(AMG_ERR_INVALID_ARG, "internal: fused extras in a program step");
+      OpJacobi<T, XS> op{};
+      record(op, XS == XS_PLAIN ? PK_JAC_PLAIN : PK_JAC_J0, Aof(l), in, Bb(l), lv.template dinv<T>(), nullptr, out,
+             double(omega), {in, Bb(l), out});
+      return;
+    }
     OpJacobi<T, XS> op{};
     op.xs = xsrc<XS>(l, in, omega);
     op.b = Bb(l);
@@ -769,6 +820,14 @@ struct Cycle {
 
   template <int XS, bool NORM>
   void resid_t(int l, const T* xp, T omega, const T* b, T* out) {
+    if (rec) {
+      static_assert(!NORM || XS == XS_PLAIN, "");
+      if (NORM || b != Bb(l)) fail(AMG_ERR_INVALID_ARG, "internal: residual form not recordable");
+      OpResid<T, T, XS, true, T, false> op{};
+      record(op, XS == XS_PLAIN ? PK_RES_PLAIN : PK_RES_J0, Aof(l), xp, Bb(l), h->levels[l].template dinv<T>(),
+             nullptr, out, double(omega), {xp, Bb(l), b, out});
+      return;
+    }
     OpResid<T, T, XS, true, T, NORM> op{};
     op.xs = xsrc<XS>(l, xp, omega);
     op.b = b;
@@ -784,6 +843,13 @@ struct Cycle {
 
   template <int BS>
   void axpy_t(const Csr& M, const T* base, T omega, int l_base, const T* x, T* out) {
+    if (rec) {
+      OpAxpy<T, BS> op{};
+      const int kind = BS == XS_ZERO ? PK_AXPY_ZERO : BS == XS_PLAIN ? PK_AXPY_PLAIN : PK_AXPY_J0;
+      record(op, kind, M, x, Bb(l_base), h->levels[l_base].template dinv<T>(), base, out, double(omega),
+             {base, Bb(l_base), x, out});
+      return;
+    }
     OpAxpy<T, BS> op{};
     op.base = xsrc<BS>(l_base, base, omega);
     op.x = x;
@@ -832,6 +898,18 @@ struct Cycle {
     const int n = h->levels[l].A.n_rows;
     const int tot = n * k;
     const int grid = std::max(1, std::min((tot + 127) / 128, dev_info().max_ctas));
+    if (rec) {
+      if (c.kind != AMG_COARSE_PINV) fail(AMG_ERR_INVALID_ARG, "internal: coarse solver not recordable");
+      PStep st{};
+      st.kind = PK_GEMV;
+      st.n_rows = n;
+      st.val = c.template m0<T>();
+      st.b = b;
+      st.out = x;
+      st.barrier = 1;
+      rec->push_back(st);
+      return;
+    }
     if (c.kind == AMG_COARSE_PINV) {
       launch(coarse_gemv<T>, grid, 128, 0, s, c.template m0<T>(), (const T*)b, x, n, k, 0, stop);
     } else if (c.kind == AMG_COARSE_LU) {
@@ -858,6 +936,19 @@ struct Cycle {
   // One visit of level l (multilevel.py:316-337).  x_zero: the incoming iterate is 0.
   // On return the new iterate is in Xb(l).
   void visit(int l, bool x_zero, char ct, int cpl) {
+    if (!rec && l > 0 && l == tail_from) {  // this level and all below: one persistent program
+      std::vector<PStep> steps;
+      rec = &steps;
+      try {
+        visit(l, x_zero, ct, cpl);
+      } catch (...) {
+        rec = nullptr;
+        throw;
+      }
+      rec = nullptr;
+      emit_program(steps);
+      return;
+    }
     const Level& lv = h->levels[l];
     const int n = lv.A.n_rows;
     T* X = Xb(l);
@@ -938,7 +1029,7 @@ LoopCtl make_ctl(Plan* pl, int maxiter);
 Red red_of(Plan* pl);
 char cycle_char(int cycle);
 void check_prec_data(amg_hierarchy* h, int prec, const Csr* A0);
-Csr override_csr(amg_hierarchy* h, const amg_csr* A0);
+Csr override_csr(amg_hierarchy* h, const amg_csr* A0, cudaStream_t s);
 void check_vec(const void* p, const char* name);
 
 struct Req {
@@ -947,7 +1038,29 @@ struct Req {
   const void* b;
   void* x;
   const Csr* A0;
+  bool program = false;  // the cycle's coarse levels may run as one persistent program
 };
+
+// First level of a cycle run as a persistent program, or -1: programs on, allowed for this
+// request, at least one level between the finest and the coarsest, a pinv coarse solve, and
+// a column layout the program's row loops cover (k = 1, or G = k / KV lanes <= 32 with
+// KV = 16 bytes when it divides k, else 1).  AMG_PROGRAM_FROM picks the level (default 1).
+template <class T>
+int tail_level(const amg_hierarchy* h, int k, bool allowed) {
+  if (!allowed || !programs_enabled()) return -1;
+  if (h->levels.size() < 3 || h->coarse.kind != AMG_COARSE_PINV) return -1;
+  if (k > 1) {
+    const int kv16 = 16 / int(sizeof(T));
+    const int kv = (k % kv16 == 0) ? kv16 : 1;
+    if ((k / kv) > 32) return -1;
+  }
+  static const int from = [] {
+    const char* e = std::getenv("AMG_PROGRAM_FROM");
+    const int v = e ? atoi(e) : 1;
+    return v >= 1 ? v : 1;
+  }();
+  return from <= int(h->levels.size()) - 2 ? from : -1;
+}
 
 std::string req_key(const char* kind, const Req& q);
 
@@ -1004,5 +1117,6 @@ unsigned long long count_f32();
 unsigned long long count_mixed();
 unsigned long long count_runtime();
 unsigned long long count_capi();
+unsigned long long count_program();
 
 }  // namespace amg

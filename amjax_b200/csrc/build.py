@@ -20,8 +20,9 @@ ROOT = PKG.parent
 OUT = PKG / "libamg_b200.so"
 OBJDIR = HERE / "_build"
 SOURCES = ["amg_runtime.cu", "amg_drv_f64.cu", "amg_drv_f32.cu", "amg_drv_mixed.cu", "amg_capi.cu",
-           "amg_noalloc.cu"]
-HEADERS = ["amg_device.cuh", "amg_runtime.cuh", "amg_pcg.cuh", "amg_drivers.cuh", str(ROOT / "include" / "amg_b200.h")]
+           "amg_noalloc.cu", "amg_program.cu"]
+HEADERS = ["amg_device.cuh", "amg_runtime.cuh", "amg_pcg.cuh", "amg_drivers.cuh", "amg_program.cuh",
+           str(ROOT / "include" / "amg_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "--expt-relaxed-constexpr", "-I", str(ROOT / "include")]

@@ -214,6 +214,15 @@ class MultilevelSolver:
         if self._handle is not None:
             lib.amg_hierarchy_destroy(self._handle)
             self._handle = None
+        descs, cd = self._native_descs()
+        h = C.c_void_p()
+        N.check(lib.amg_hierarchy_create(descs, len(descs), C.byref(cd), C.byref(h)))
+        self._handle = h
+        self._handle_key = key
+        return h
+
+    def _native_descs(self):
+        """The C-ABI level and coarse-solver descriptors over this hierarchy's device arrays."""
         L = len(self.levels)
         if L < 2:
             raise ValueError("a single-level hierarchy has no multigrid cycle (AMJax's _cycle needs >= 2 levels)")
@@ -240,11 +249,7 @@ class MultilevelSolver:
         for slot in ("m0_64", "m0_32", "m1_64", "m1_32", "perm"):
             t = nat.get(slot)
             setattr(cd, slot, t.data_ptr() if t is not None else None)
-        h = C.c_void_p()
-        N.check(lib.amg_hierarchy_create(descs, L, C.byref(cd), C.byref(h)))
-        self._handle = h
-        self._handle_key = key
-        return h
+        return descs, cd
 
     def _precision(self, precision):
         if precision is None:

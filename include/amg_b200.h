@@ -14,6 +14,12 @@
  *    the legacy default stream).
  *  - Functions return an ``amg_status``; no C++ exception crosses the ABI.
  *    ``amg_last_error()`` gives a human-readable message for the calling thread.
+ *  - Matrix structure is checked on the device before use: by amg_hierarchy_create for
+ *    the hierarchy, on every call for an A0 override, and the first time a stand-alone
+ *    kernel (amg_jacobi, amg_spmv, amg_inverse_diagonal, amg_sampled_outer) sees a matrix
+ *    (same pointers and sizes: a structure changed in place later is not re-checked).  The
+ *    check waits for its verdict on the call's stream and is skipped while that stream is
+ *    being captured into a CUDA graph.  A bad structure gives AMG_ERR_BAD_MATRIX.
  *  - Non-convergence is not an error (the reference returns x silently,
  *    amjax/multilevel.py:414-425); per-column iteration counts and final relative
  *    residuals are reported through ``iters_out`` / ``relres_out`` (host arrays of
@@ -114,7 +120,10 @@ typedef struct amg_hierarchy amg_hierarchy;
 
 /* Create a hierarchy handle over caller-owned device arrays (the arrays uploaded once
  * by MultilevelSolver.from_pyamg, amjax/multilevel.py:125-186 / _convert_hierarchy
- * :557-590).  Validates sizes; the arrays are not copied. */
+ * :557-590).  Validates sizes, and the structure of every A, P and R on the device (row
+ * pointers start at 0, never decrease and end at nnz; columns in [0, n_cols); columns
+ * need not be sorted within a row): AMG_ERR_BAD_MATRIX otherwise.  Waits for the device
+ * first.  The arrays are not copied. */
 amg_status amg_hierarchy_create(const amg_level_desc* levels, int32_t n_levels,
                                 const amg_coarse_desc* coarse, amg_hierarchy** out);
 amg_status amg_hierarchy_destroy(amg_hierarchy* h);
