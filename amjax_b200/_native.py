@@ -66,6 +66,8 @@ SIGNATURES = {
     "amg_inverse_diagonal": (C.c_int, [C.POINTER(amg_csr), C.c_int32, C.c_void_p, C.c_void_p]),
     "amg_sampled_outer": (C.c_int, [C.POINTER(amg_csr), C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                     C.c_void_p]),
+    "amg_time_pcg_ops": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_char_p, C.c_int32,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "amg_kernel_launch_count": (C.c_int64, []),
     "amg_last_error": (C.c_char_p, []),
     "amg_version": (C.c_char_p, []),
@@ -116,6 +118,19 @@ def check(status: int):
 def call(name, *args):
     lib = load()
     check(getattr(lib, name)(*args))
+
+
+def time_pcg_ops(handle, k, reps=5, stream=None):
+    """Per-kernel timing of one mixed-precision PCG step's fine-level kernels
+    (``amg_time_pcg_ops``): a list of (name, microseconds per launch, algorithmic bytes)."""
+    m, width = 16, 64
+    names = C.create_string_buffer(m * width)
+    us = (C.c_double * m)()
+    by = (C.c_double * m)()
+    n = C.c_int32()
+    call("amg_time_pcg_ops", handle, int(k), int(reps), stream_ptr(stream), m, names, width, us, by, C.byref(n))
+    raw = names.raw
+    return [(raw[i * width:(i + 1) * width].split(b"\0", 1)[0].decode(), us[i], by[i]) for i in range(n.value)]
 
 
 def kernel_launch_count() -> int:

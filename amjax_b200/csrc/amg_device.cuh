@@ -47,6 +47,19 @@ __device__ __forceinline__ size_t voff(int j, int ld, int c) {
 }
 
 
+// Arithmetic with its rounding spelled out.  Every multiply, add and fused multiply-add in
+// the ops goes through these, so no kernel's compilation can pick a different contraction
+// (a*b + c*d can fuse either product) and every kernel that runs an op -- any lane layout,
+// the launched kernels or the persistent program -- rounds it the same way.
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // 32-byte accesses (sm_100: one 256-bit load or store per thread), used by the wide lean
 // kernel; the address must be 32-byte aligned (the launch configuration checks every
 // pointer and the row stride).  The load takes the read-only path: every CSR-op operand
@@ -282,11 +295,11 @@ csr_k1(const int* __restrict__ rowptr, const int* __restrict__ col,
     const bool valid = row < n_rows;
     if (valid) {
       const int s = __ldg(rowptr + row), e = __ldg(rowptr + row + 1);
-      for (int nz = s + lane; nz < e; nz += G) acc += static_cast<A>(__ldg(val + nz)) * op.x1(__ldg(col + nz));
+      for (int nz = s + lane; nz < e; nz += G) acc = rfma(static_cast<A>(__ldg(val + nz)), op.x1(__ldg(col + nz)), acc);
     }
     if constexpr (G > 1) {
 #pragma unroll
-      for (int off = G >> 1; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+      for (int off = G >> 1; off > 0; off >>= 1) acc = radd(acc, __shfl_xor_sync(0xffffffffu, acc, off, G));
     }
     if (valid && lane == 0) red += op.epi1(row, acc);
   }
@@ -661,7 +674,7 @@ struct XSource {
   int ld;
   __device__ __forceinline__ T get1(int j) const {
     if constexpr (XS == XS_PLAIN) return __ldg(x + j);
-    else if constexpr (XS == XS_JAC0) return omega * (__ldg(dinv + j) * __ldg(b + j));
+    else if constexpr (XS == XS_JAC0) return rmul(omega, rmul(__ldg(dinv + j), __ldg(b + j)));
     else return T(0);
   }
   template <int KV>
@@ -673,7 +686,7 @@ struct XSource {
       ld_vec<T, KV>(b + voff(j, ld, c0), bv);
       const T d = __ldg(dinv + j);
 #pragma unroll
-      for (int i = 0; i < KV; ++i) v[i] = omega * (d * bv[i]);
+      for (int i = 0; i < KV; ++i) v[i] = rmul(omega, rmul(d, bv[i]));
     } else {
 #pragma unroll
       for (int i = 0; i < KV; ++i) v[i] = T(0);
@@ -716,13 +729,13 @@ struct OpJacobi {
 
   __device__ __forceinline__ double epi1(int i, T s) const {
     const T xv = xs.get1(i);
-    const T r = __ldg(b + i) - s;
-    const T temp = __ldg(dinv + i) * r + xv;
-    const T y = (T(1) - omega) * xv + omega * temp;
+    const T r = rsub(__ldg(b + i), s);
+    const T temp = rfma(__ldg(dinv + i), r, xv);
+    const T y = rfma(omega, temp, rmul(rsub(T(1), omega), xv));
     if (!active || active[0]) out[i] = y;
-    if (norm) return (double)r * (double)r;
-    if (rdot64) return __ldg(rdot64 + i) * (double)y;
-    if (rdot32) return (double)__ldg(rdot32 + i) * (double)y;
+    if (norm) return rmul((double)r, (double)r);
+    if (rdot64) return rmul(__ldg(rdot64 + i), (double)y);
+    if (rdot32) return rmul((double)__ldg(rdot32 + i), (double)y);
     return 0.0;
   }
   template <int KV>
@@ -736,11 +749,12 @@ struct OpJacobi {
   __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& p,
                                        double (&red)[KV]) const {
     T y[KV], r[KV];
+    const T om1 = rsub(T(1), omega);
 #pragma unroll
     for (int v = 0; v < KV; ++v) {
-      r[v] = p.b[v] - s[v];
-      const T temp = p.d * r[v] + p.x[v];
-      y[v] = (T(1) - omega) * p.x[v] + omega * temp;
+      r[v] = rsub(p.b[v], s[v]);
+      const T temp = rfma(p.d, r[v], p.x[v]);
+      y[v] = rfma(omega, temp, rmul(om1, p.x[v]));
     }
     const size_t o = voff(i, ld, c0);
     if (!(norm | (rdot64 != nullptr) | (rdot32 != nullptr) | (active != nullptr))) {
@@ -749,17 +763,17 @@ struct OpJacobi {
     }
     if (norm) {
 #pragma unroll
-      for (int v = 0; v < KV; ++v) red[v] += (double)r[v] * (double)r[v];
+      for (int v = 0; v < KV; ++v) red[v] = rfma((double)r[v], (double)r[v], red[v]);
     } else if (rdot64) {
       double rv[KV];
       ld_vec<double, KV>(rdot64 + o, rv);
 #pragma unroll
-      for (int v = 0; v < KV; ++v) red[v] += rv[v] * (double)y[v];
+      for (int v = 0; v < KV; ++v) red[v] = rfma(rv[v], (double)y[v], red[v]);
     } else if (rdot32) {
       float rv[KV];
       ld_vec<float, KV>(rdot32 + o, rv);
 #pragma unroll
-      for (int v = 0; v < KV; ++v) red[v] += (double)rv[v] * (double)y[v];
+      for (int v = 0; v < KV; ++v) red[v] = rfma((double)rv[v], (double)y[v], red[v]);
     }
     if (active) {
 #pragma unroll
@@ -807,10 +821,10 @@ struct OpResid {
   template <int KV>
   __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const { xs.template getk<KV>(j, c0, v); }
   __device__ __forceinline__ double epi1(int i, T s) const {
-    const T r = __ldg(b + i) - s;
+    const T r = rsub(__ldg(b + i), s);
     if constexpr (STORE) out[i] = r;
     if (out_lo) out_lo[i] = static_cast<TLO>(r);
-    return NORM ? (double)r * (double)r : 0.0;
+    return NORM ? rmul((double)r, (double)r) : 0.0;
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& p) const {
@@ -822,8 +836,8 @@ struct OpResid {
     T r[KV];
 #pragma unroll
     for (int v = 0; v < KV; ++v) {
-      r[v] = p.b[v] - s[v];
-      if constexpr (NORM) red[v] += (double)r[v] * (double)r[v];
+      r[v] = rsub(p.b[v], s[v]);
+      if constexpr (NORM) red[v] = rfma((double)r[v], (double)r[v], red[v]);
     }
     if constexpr (STORE) st_vec<T, KV>(out + voff(i, ld, c0), r);
     if (out_lo) {
@@ -868,7 +882,7 @@ struct OpAxpy {
     ld_vec<T, KV>(x + voff(j, ld, c0), v);
   }
   __device__ __forceinline__ double epi1(int i, T s) const {
-    out[i] = base.get1(i) + s;
+    out[i] = radd(base.get1(i), s);
     return 0.0;
   }
   template <int KV>
@@ -880,7 +894,7 @@ struct OpAxpy {
                                        double (&)[KV]) const {
     T y[KV];
 #pragma unroll
-    for (int v = 0; v < KV; ++v) y[v] = p.x[v] + s[v];
+    for (int v = 0; v < KV; ++v) y[v] = radd(p.x[v], s[v]);
     st_vec<T, KV>(out + voff(i, ld, c0), y);
   }
   __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
@@ -943,7 +957,7 @@ struct OpCgQDir {
   __device__ __forceinline__ double epi1(int i, T s) const {
     const T pn = x1(i);
     p_new[i] = pn;
-    return (double)pn * (double)s;
+    return rmul((double)pn, (double)s);
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
@@ -953,7 +967,7 @@ struct OpCgQDir {
   __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& pp,
                                        double (&red)[KV]) const {
 #pragma unroll
-    for (int v = 0; v < KV; ++v) red[v] += (double)pp.x[v] * (double)s[v];
+    for (int v = 0; v < KV; ++v) red[v] = rfma((double)pp.x[v], (double)s[v], red[v]);
     st_vec<T, KV>(p_new + voff(i, ld, c0), pp.x);
   }
   __device__ __forceinline__ int finalize_col(int c, double s) const {
@@ -993,12 +1007,12 @@ struct OpCgUpdA {
     T rv = r[i];
     if (active[0]) {
       const T a = static_cast<T>(alpha[0]);
-      x[i] = x[i] + a * __ldg(p + i);
-      rv = rv - a * s;
+      x[i] = rfma(a, __ldg(p + i), x[i]);
+      rv = rfma(-a, s, rv);
       r[i] = rv;
     }
     if (r_lo) r_lo[i] = static_cast<TLO>(rv);
-    return (double)rv * (double)rv;
+    return rmul((double)rv, (double)rv);
   }
   template <int KV>
   __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
@@ -1019,11 +1033,11 @@ struct OpCgUpdA {
       rv[v] = pp.c[v];
       if (active[c0 + v]) {
         const T a = static_cast<T>(alpha[c0 + v]);
-        xv[v] = xv[v] + a * pp.x[v];
-        rv[v] = rv[v] - a * s[v];
+        xv[v] = rfma(a, pp.x[v], xv[v]);
+        rv[v] = rfma(-a, s[v], rv[v]);
         any = true;
       }
-      red[v] += (double)rv[v] * (double)rv[v];
+      red[v] = rfma((double)rv[v], (double)rv[v], red[v]);
     }
     if (any) {
       st_vec<T, KV>(x + o, xv);
@@ -1068,7 +1082,7 @@ struct OpFold {
     ld_vec<TS, KV>(xs + o, sv);
 #pragma unroll
     for (int v = 0; v < KV; ++v) {
-      xv[v] += static_cast<T>(sv[v]);
+      xv[v] = radd(xv[v], static_cast<T>(sv[v]));
       zero[v] = TS(0);
     }
     st_vec<T, KV>(x + o, xv);
@@ -1111,15 +1125,15 @@ struct OpCgUpdate {
       for (int v = 0; v < KV; ++v) {
         if (active[c0 + v]) {
           const T a = static_cast<T>(alpha[c0 + v]);
-          xv[v] = xv[v] + a * pv[v];
-          rv[v] = rv[v] - a * qv[v];
+          xv[v] = rfma(a, pv[v], xv[v]);
+          rv[v] = rfma(-a, qv[v], rv[v]);
         }
       }
       st_vec<T, KV>(x + o, xv);
       st_vec<T, KV>(r + o, rv);
     }
 #pragma unroll
-    for (int v = 0; v < KV; ++v) red[v] += (double)rv[v] * (double)rv[v];
+    for (int v = 0; v < KV; ++v) red[v] = rfma((double)rv[v], (double)rv[v], red[v]);
     if (r_lo) {
       TLO rl[KV];
 #pragma unroll
@@ -1151,7 +1165,7 @@ struct OpRefine {
     ld_cvt<T, TE, KV>(e + o, ev);
 #pragma unroll
     for (int v = 0; v < KV; ++v)
-      if (active[c0 + v]) xv[v] += ev[v];
+      if (active[c0 + v]) xv[v] = radd(xv[v], ev[v]);
     st_vec<T, KV>(x + o, xv);
   }
   __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
@@ -1177,7 +1191,7 @@ struct OpJac0 {
     ld_vec<T, KV>(b + o, bv);
     const T d = __ldg(dinv + i);
 #pragma unroll
-    for (int v = 0; v < KV; ++v) bv[v] = omega * (d * bv[v]);
+    for (int v = 0; v < KV; ++v) bv[v] = rmul(omega, rmul(d, bv[v]));
     st_vec<T, KV>(out + o, bv);
   }
   __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
@@ -1215,7 +1229,7 @@ struct OpSetup {
     T v[KV];
     ld_vec<T, KV>(src + o, v);
 #pragma unroll
-    for (int j = 0; j < KV; ++j) red[j] += (double)v[j] * (double)v[j];
+    for (int j = 0; j < KV; ++j) red[j] = rfma((double)v[j], (double)v[j], red[j]);
     if (dst) st_vec<T, KV>(dst + o, v);
     if (dst_lo) {
       TLO l[KV];
@@ -1281,7 +1295,7 @@ struct OpMaskCopy {
       TR rv[KV];
       ld_vec<TR, KV>(rdot + o, rv);
 #pragma unroll
-      for (int j = 0; j < KV; ++j) red[j] += (double)rv[j] * (double)v[j];
+      for (int j = 0; j < KV; ++j) red[j] = rfma((double)rv[j], (double)v[j], red[j]);
     }
     if (active) {
 #pragma unroll
@@ -1335,9 +1349,9 @@ __global__ void coarse_gemv(const T* __restrict__ M, const T* __restrict__ b, T*
     const int i = t / k, c = t % k;
     T s = T(0);
     if (!transpose) {
-      for (int j = 0; j < n; ++j) s += M[(size_t)i * n + j] * b[(size_t)j * k + c];
+      for (int j = 0; j < n; ++j) s = rfma(M[(size_t)i * n + j], b[(size_t)j * k + c], s);
     } else {
-      for (int j = 0; j < n; ++j) s += M[(size_t)j * n + i] * b[(size_t)j * k + c];
+      for (int j = 0; j < n; ++j) s = rfma(M[(size_t)j * n + i], b[(size_t)j * k + c], s);
     }
     x[(size_t)i * k + c] = s;
   }
@@ -1356,13 +1370,13 @@ __global__ void coarse_trsv(const T* __restrict__ LU, const int* __restrict__ pe
       for (int i = 0; i < n; ++i) x[(size_t)i * k + c] = b[(size_t)perm[i] * k + c];
       for (int i = 0; i < n; ++i) {
         T s = x[(size_t)i * k + c];
-        for (int j = 0; j < i; ++j) s -= LU[(size_t)i * n + j] * x[(size_t)j * k + c];
+        for (int j = 0; j < i; ++j) s = rfma(-LU[(size_t)i * n + j], x[(size_t)j * k + c], s);
         x[(size_t)i * k + c] = s;
       }
     }
     for (int i = n - 1; i >= 0; --i) {
       T s = x[(size_t)i * k + c];
-      for (int j = i + 1; j < n; ++j) s -= LU[(size_t)i * n + j] * x[(size_t)j * k + c];
+      for (int j = i + 1; j < n; ++j) s = rfma(-LU[(size_t)i * n + j], x[(size_t)j * k + c], s);
       x[(size_t)i * k + c] = s / LU[(size_t)i * n + i];
     }
   }

@@ -26,7 +26,13 @@ __global__ void __launch_bounds__(kBlock) program_kernel(const Program p, int k,
 int program_grid(bool f64) {
   const void* fn = f64 ? reinterpret_cast<const void*>(program_kernel<double>)
                        : reinterpret_cast<const void*>(program_kernel<float>);
-  return dev_info().nsm * resident_ctas(fn, 0);
+  static const int per_sm_cap = [] {  // AMG_PROGRAM_CTAS: CTAs per SM (default: all that fit)
+    const char* e = std::getenv("AMG_PROGRAM_CTAS");
+    const int v = e ? atoi(e) : 0;
+    return v > 0 ? v : 64;
+  }();
+  const int per_sm = std::min(resident_ctas(fn, 0), per_sm_cap);
+  return std::min(dev_info().nsm * per_sm, kBarMaxCtas);
 }
 
 void launch_program(const Program& p, bool f64, int k, const int* stop, const GridBar& gb, cudaStream_t s) {

@@ -60,10 +60,18 @@ struct Program {
   PStep steps[kMaxSteps];
 };
 
+// Barrier state: a top-level count, the generation, the status word, then one count per
+// group of kBarGroup consecutive CTAs, kBarStride words apart (own 128-byte line each).
+constexpr int kBarGroup = 8;
+constexpr int kBarStride = 32;
+constexpr int kBarMaxCtas = 2048;
+constexpr int kBarWords = 4 + kBarStride * (kBarMaxCtas / kBarGroup);
+
 struct GridBar {
-  unsigned* count;   // CTAs arrived at the current barrier
+  unsigned* count;   // groups arrived at the current barrier
   unsigned* gen;     // barrier generation
   int* status;       // nonzero: a wait ran out (the launch gave up)
+  unsigned* groups;  // per-group arrival counts
   long long limit;   // clock64 budget of one wait
 };
 
@@ -73,8 +81,11 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   return v;
 }
 
-// Grid-wide barrier of a cooperative launch (every CTA resident).  Returns false when a
-// wait ran out here or in another CTA; the caller then returns.
+// Grid-wide barrier of a cooperative launch (every CTA resident), two levels: the CTAs of
+// a group of kBarGroup arrive on the group's own counter, and the last of each group
+// arrives on the top-level counter for all of them (one contended atomic per group, not
+// per CTA); the last group bumps the generation that every CTA waits on.  Returns false
+// when a wait ran out here or in another CTA; the caller then returns.
 __device__ __forceinline__ bool grid_sync(const GridBar& gb) {
   __shared__ int s_ok;
   __syncthreads();
@@ -82,8 +93,18 @@ __device__ __forceinline__ bool grid_sync(const GridBar& gb) {
     int ok = *reinterpret_cast<volatile int*>(gb.status) == 0;
     if (ok) {
       const unsigned g0 = ld_acquire_u32(gb.gen);
+      const unsigned grp = blockIdx.x / kBarGroup;
+      const unsigned gsize = min(unsigned(kBarGroup), gridDim.x - grp * kBarGroup);
+      const unsigned ngroups = (gridDim.x + kBarGroup - 1) / kBarGroup;
+      unsigned* gc = gb.groups + size_t(grp) * kBarStride;
       __threadfence();
-      if (atomicAdd(gb.count, 1u) == gridDim.x - 1) {
+      bool last = false;
+      if (atomicAdd(gc, 1u) == gsize - 1) {
+        atomicExch(gc, 0u);
+        __threadfence();
+        last = atomicAdd(gb.count, 1u) == ngroups - 1;
+      }
+      if (last) {
         atomicExch(gb.count, 0u);
         __threadfence();
         atomicAdd(gb.gen, 1u);
@@ -123,9 +144,9 @@ __device__ __forceinline__ void prog_rows1(const Op& op, const PStep& st, int gt
     const bool valid = row < st.n_rows;
     if (valid) {
       const int s = __ldg(st.rowptr + row), e = __ldg(st.rowptr + row + 1);
-      for (int nz = s + lane; nz < e; nz += G) acc += static_cast<A>(__ldg(val + nz)) * op.x1(__ldg(st.col + nz));
+      for (int nz = s + lane; nz < e; nz += G) acc = rfma(static_cast<A>(__ldg(val + nz)), op.x1(__ldg(st.col + nz)), acc);
     }
-    for (int off = G >> 1; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, G);
+    for (int off = G >> 1; off > 0; off >>= 1) acc = radd(acc, __shfl_xor_sync(0xffffffffu, acc, off, G));
     if (valid && lane == 0) op.epi1(row, acc);
   }
 }
@@ -248,7 +269,7 @@ __device__ void prog_step(const PStep& st, int k, int gtid, int nth) {
       for (int t = gtid; t < n * k; t += nth) {
         const int i = t / k, c = t % k;
         T s = T(0);
-        for (int j = 0; j < n; ++j) s += M[(size_t)i * n + j] * b[(size_t)j * k + c];
+        for (int j = 0; j < n; ++j) s = rfma(M[(size_t)i * n + j], b[(size_t)j * k + c], s);
         out[(size_t)i * k + c] = s;
       }
       break;

@@ -279,8 +279,8 @@ Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s) {
   pl->counter = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * (1 + kRedGroups)));
   CK(cudaMemset(pl->counter, 0, sizeof(unsigned) * (1 + kRedGroups)));
   CK(cudaHostAlloc(reinterpret_cast<void**>(&pl->h_stop), sizeof(int), cudaHostAllocDefault));
-  pl->bar = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * 4));
-  CK(cudaMemset(pl->bar, 0, sizeof(unsigned) * 4));
+  pl->bar = static_cast<unsigned*>(pl->alloc(sizeof(unsigned) * kBarWords));
+  CK(cudaMemset(pl->bar, 0, sizeof(unsigned) * kBarWords));
   Plan* raw = pl.get();
   h->plans[key] = std::move(pl);
   return raw;
@@ -352,7 +352,7 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
                      const Emit& body, const Emit& epilogue, bool has_loop, int gmax) {
   const ExecMode mode = exec_mode();
   if (mode == EXEC_EAGER) {
-    CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * 3, user));
+    CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * kBarWords, user));
     prologue(user);
     if (has_loop) {
       for (int trip = 0;; ++trip) {
@@ -432,7 +432,7 @@ void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& p
     ge = pl->graphs.front().second.get();
   }
   if (pl->used_program)  // barrier count, generation and status start at 0
-    CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * 3, user));
+    CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * kBarWords, user));
   if (!ge->host_loop) {
     CK(cudaGraphLaunch(ge->exec, user));
   } else {
@@ -519,7 +519,7 @@ void read_results(Plan* pl, cudaStream_t s, bool cg, int32_t* iters_out, double*
     CK(cudaMemcpyAsync(&st, pl->bar + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (st) {
-      CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * 3, s));
+      CK(cudaMemsetAsync(pl->bar, 0, sizeof(unsigned) * kBarWords, s));
       fail(AMG_ERR_TIMEOUT, "a grid barrier of the persistent coarse-level kernel ran out of time "
                             "(AMG_SPIN_LIMIT); the result is not valid");
     }

@@ -738,7 +738,7 @@ struct Cycle {
 
   // Run the recorded steps: one cooperative launch per kMaxSteps steps.
   void emit_program(const std::vector<PStep>& steps) {
-    const GridBar gb{pl->bar, pl->bar + 1, reinterpret_cast<int*>(pl->bar + 2), spin_limit()};
+    const GridBar gb{pl->bar, pl->bar + 1, reinterpret_cast<int*>(pl->bar + 2), pl->bar + 4, spin_limit()};
     for (size_t i0 = 0; i0 < steps.size(); i0 += kMaxSteps) {
       Program p{};
       p.nsteps = int(std::min<size_t>(kMaxSteps, steps.size() - i0));

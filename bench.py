@@ -15,8 +15,8 @@ Timing: W untimed warm-up solves, then K solves each bracketed by CUDA events on
 launching stream, with a 256 MB L2 flush between solves outside the events; barrier +
 synchronize around the timed block; max over ranks.  ``e2e`` repeats the headline
 through the public API from pinned host buffers (H2D of B and D2H of X inside the
-timed region).  ``roofline`` times the dominant kernel (the fine-level fused Jacobi
-sweep, FP32, k = 64) alone through the C ABI.  ``cpu_baseline`` times the FP64 CPU
+timed region).  ``roofline`` times every fine-level kernel of the CG step alone through
+the C ABI (``amg_time_pcg_ops``) and reports the one with the largest time per solve.  ``cpu_baseline`` times the FP64 CPU
 oracle (numpy/scipy restatement of AMJax's solve) on all k columns, one thread.
 ``--impl reference`` times that CPU restatement instead: all k columns per step, one
 column per task over one single-threaded worker process per host core, set-up outside
@@ -393,41 +393,33 @@ def run_ours(args):
         var["speedup_mixed_f64cg_vs_f64_k64_pcg"] = var["k64_pcg_f64"]["ms"] / var["k64_pcg_mixed_f64cg"]["ms"]
         out["variants"] = var
 
-    # ---- roofline: dominant kernel (fine-level fused Jacobi sweep, FP32, k) timed alone
-    lvl0 = ml.levels[0]
-    xs = torch.randn(Nn, k, dtype=torch.float32, device="cuda")
-    bs = torch.randn(Nn, k, dtype=torch.float32, device="cuda")
-    ys = torch.empty_like(xs)
-    d = lvl0.A.desc()
-    sp_ = N.stream_ptr()
-
-    def jac():
-        N.call("amg_jacobi", d, 1, N.ptr(xs), N.ptr(bs), N.ptr(lvl0.Dinv32), N.ptr(ys), k, 1, 2.0 / 3.0, sp_)
-
-    reps = 50
-    for _ in range(5):
-        jac()
-    torch.cuda.synchronize()
-    s0 = torch.cuda.Event(enable_timing=True)
-    s1 = torch.cuda.Event(enable_timing=True)
-    s0.record()
-    for _ in range(reps):
-        jac()
-    s1.record()
-    torch.cuda.synchronize()
-    t_launch = s0.elapsed_time(s1) / reps * 1e-3
-    jb = bytemodel.jacobi_sweep_bytes(Nn, lvl0.A.nnz, k, 4)
-    achieved = jb / t_launch / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "jacobi_fp32_k64_poisson500.json")
+    # ---- roofline: every fine-level kernel of the headline's CG step timed alone with CUDA
+    # events (layouts as in the solve, L2 evicted before each launch); the dominant one is
+    # the kernel with the largest time per solve (microseconds x launches per solve)
+    it = max(its)
+    per_solve = {"cg_direction_pAp": it, "cg_update": it, "post_smooth_with_dot": it + 1,
+                 "residual_presmoothed": it + 1, "restriction": it + 1, "prolongation_correction": it + 1}
+    rows = N.time_pcg_ops(ml._native(), k, reps=10)
+    traffic_db = {}
+    tpath = os.path.join(ROOT, "profiles", "pcg_mixed_k64_kernels_dram.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
-    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                       "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind + " (burst copy)",
-                       "kernel": "csr_kb / csr_kr <OpJacobi<float,XS_PLAIN>> (autotuned kernel and layout): fine-level fused "
-                                 f"Jacobi sweep, FP32, k={k}, N={Nn}",
-                       "algorithmic_bytes_per_launch": jb, "launch_us": t_launch * 1e6}
+            traffic_db = json.load(f).get("dram_bytes_per_launch", {})
+    table = []
+    for name, us_, by in rows:
+        gbs = by / (us_ * 1e-6) / 1e9
+        table.append({"kernel": name, "us": us_, "algorithmic_bytes": by, "gbs": gbs, "frac": gbs / hbm_peak,
+                      "launches_per_solve": per_solve.get(name), "dram_bytes_ncu": traffic_db.get(name)})
+    dom = max((r for r in table if r["launches_per_solve"]), key=lambda r: r["us"] * r["launches_per_solve"])
+    out["roofline"] = {"bound": "hbm", "achieved": dom["gbs"], "peak": hbm_peak, "unit": "GB/s",
+                       "frac": dom["frac"], "traffic": dom["dram_bytes_ncu"],
+                       "peak_kind": peak_kind + " (burst copy)",
+                       "kernel": f"{dom['kernel']} (fine level, N={Nn}, k={k}, FP32 vectors; the largest "
+                                 f"microseconds x launches per solve)",
+                       "algorithmic_bytes_per_launch": dom["algorithmic_bytes"], "launch_us": dom["us"],
+                       "timing": "each launch alone between CUDA events on the launching stream, after a "
+                                 "256 MB write that evicts L2; mean of 10",
+                       "kernels": table}
 
     ck = clocks.stop(bus)
     out["clocks"] = ck

@@ -203,6 +203,19 @@ amg_status amg_inverse_diagonal(const amg_csr* A, int32_t dtype, void* dinv, voi
 amg_status amg_sampled_outer(const amg_csr* A, const double* lam, const double* x, int32_t k,
                              double* grad, void* stream);
 
+/* Diagnostic, no counterpart in the reference: times, on `stream`, each fine-level fused
+ * kernel of one mixed-precision (reliable-update) PCG step for k right-hand sides -- the
+ * <p, A p> pass with the direction update, the CG update, the post-smoothing sweep with
+ * the fused <r, z>, the residual of the pre-smoothed iterate, restriction, prolongation
+ * with correction, the FP64 true residual and the increment fold -- with the layouts the
+ * solve uses (tuned first if not yet).  Each of `reps` launches is timed alone with CUDA
+ * events after a write that evicts L2.  Writes up to max_ops rows: a NUL-terminated name
+ * (name_len bytes per row), the mean microseconds per launch and the kernel's algorithmic
+ * bytes (every operand read or written once); *n_ops = rows written.  Uses the hierarchy's
+ * mixed-precision scratch for k, so it must not overlap a solve on the same hierarchy. */
+amg_status amg_time_pcg_ops(amg_hierarchy* h, int32_t k, int32_t reps, void* stream, int32_t max_ops,
+                            char* names, int32_t name_len, double* us, double* bytes, int32_t* n_ops);
+
 /* Number of kernels this library launched in the calling process (monotone counter;
  * one CUDA-graph launch counts every kernel node it contains). */
 int64_t amg_kernel_launch_count(void);

@@ -68,8 +68,8 @@ def test_program_path_is_bit_identical_to_launches():
     fewer = with_prog.pop("launches")
     more = without.pop("launches")
     assert set(with_prog) == set(without)
-    for key in with_prog:
-        assert with_prog[key] == without[key], key
+    differ = [key for key in with_prog if with_prog[key] != without[key]]
+    assert not differ, differ
     assert fewer < more  # the program replaced launches
 
 
