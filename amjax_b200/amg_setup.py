@@ -21,6 +21,18 @@ Algorithms (restated from the literature, not from PyAMG's source):
 * Ruge-Stueben classical AMG (Ruge & Stueben, 1987): classical strength with
   ``theta = 0.25`` on ``|a_ij|``, the first-pass C/F splitting, direct interpolation,
   ``R = P^T``, Galerkin coarse operators.
+* Root-node AMG (Manteuffel, Olson, Schroder & Southworth, SISC 39, 2017), with the
+  energy-minimising prolongation of Olson, Schroder & Tuminaro (Num. Lin. Alg. Appl. 18,
+  2011): standard aggregation with one root node per aggregate; a tentative prolongator
+  that injects at the root nodes (``P[root_j, :] = e_j``) and reproduces the candidate
+  (``P B_c = B``); then a few Jacobi-preconditioned CG iterations on ``trace(P^T A P)``
+  over the sparsity pattern of ``A^degree T`` with both constraints kept (``degree = 2``,
+  ``maxiter = 4``).
+* Pairwise aggregation (Notay, ETNA 37, 2010): two passes of pairing each node with its
+  most negatively coupled free neighbour among the strong ones (``a_ij < -beta max_k
+  |a_ik|``, ``beta = 0.25``; strongly diagonally dominant rows stay out of the coarse
+  grid), so aggregates hold at most four nodes; unsmoothed piecewise-constant
+  prolongator, ``R = P^T``.
 
 The resulting arrays are NOT bit-identical to PyAMG's (tie-breaking and the spectral
 radius estimate differ); the solve phase only needs some valid hierarchy, and the GPU
@@ -41,6 +53,8 @@ __all__ = [
     "smoothed_aggregation_solver",
     "ruge_stuben_solver",
     "air_solver",
+    "rootnode_solver",
+    "pairwise_solver",
     "save_hierarchy",
     "load_hierarchy",
 ]
@@ -128,14 +142,15 @@ def _symmetric_strength(A, theta=0.0):
     return _csr(S)
 
 
-def _standard_aggregation(S):
+def _standard_aggregation(S, return_roots=False):
     """Greedy three-pass aggregation on the strength graph S (diagonal-free CSR).
 
     Pass 1: every node whose neighbours are all free becomes a root; it and its
     neighbours form an aggregate.  Pass 2: each still-free node joins the aggregate of
     an aggregated neighbour.  Pass 3: each node still free starts a new aggregate with
-    its free neighbours.  Nodes without neighbours stay unaggregated (index -1).
-    Returns (agg index per node, number of aggregates).
+    its free neighbours (it is that aggregate's root).  Nodes without neighbours stay
+    unaggregated (index -1).  Returns (agg index per node, number of aggregates), and
+    with ``return_roots`` also the root node of every aggregate.
     """
     n = S.shape[0]
     ptr, idx = S.indptr, S.indices
@@ -143,6 +158,7 @@ def _standard_aggregation(S):
     deg = np.diff(ptr)
     agg[deg == 0] = -1
     nagg = 0
+    roots = []
     ptr_l = ptr.tolist(); idx_l = idx.tolist(); agg_l = agg.tolist()
     for i in range(n):
         if agg_l[i] != -2:
@@ -152,6 +168,7 @@ def _standard_aggregation(S):
             agg_l[i] = nagg
             for j in nb:
                 agg_l[j] = nagg
+            roots.append(i)
             nagg += 1
     pass2 = agg_l[:]
     for i in range(n):
@@ -169,7 +186,10 @@ def _standard_aggregation(S):
         for j in idx_l[ptr_l[i]:ptr_l[i + 1]]:
             if agg_l[j] == -2:
                 agg_l[j] = nagg
+        roots.append(i)
         nagg += 1
+    if return_roots:
+        return np.asarray(agg_l, dtype=np.int64), nagg, np.asarray(roots, dtype=np.int64)
     return np.asarray(agg_l, dtype=np.int64), nagg
 
 
@@ -224,6 +244,164 @@ def smoothed_aggregation_solver(A, B=None, max_levels=10, max_coarse=10, theta=0
         levels.append(HostLevel(Ac))
         B = Bc
     return HostHierarchy(levels, kind="smoothed_aggregation")
+
+
+# ---------------------------------------------------------------- root node
+
+def _rootnode_tentative(agg, nagg, roots, B):
+    """Tentative prolongator that injects at the root nodes: T[i, agg_i] = B_i / B_root,
+    so T[root_j, :] = e_j and T B_c = B on aggregated rows, with B_c = B at the roots."""
+    n = B.shape[0]
+    b = B[:, 0]
+    broot = b[roots]
+    broot = np.where(broot != 0, broot, 1.0)
+    member = agg >= 0
+    rows = np.nonzero(member)[0]
+    cols = agg[member]
+    T = sp.csr_matrix((b[member] / broot[cols], (rows, cols)), shape=(n, nagg))
+    return _csr(T), broot.reshape(-1, 1)
+
+
+def _energy_prolongation(A, T, Bc, roots, free_rows, degree=2, maxiter=4):
+    """Energy-minimising prolongator (Olson, Schroder & Tuminaro 2011): CG on
+    ``trace(P^T A P)`` from ``P = T`` over corrections D that keep (1) the sparsity pattern
+    of ``A^degree T``, (2) the root rows fixed (D[roots, :] = 0), (3) the candidate,
+    ``D B_c = 0`` row by row; Jacobi (D^-1) preconditioned, Frobenius inner products."""
+    n = A.shape[0]
+    Pat = abs(T).tocsr()
+    for _ in range(degree):
+        Pat = abs(A) @ Pat
+    Pat = _csr(Pat + abs(T))
+    Pat.data[:] = 1.0
+    keep = np.zeros(n)
+    keep[free_rows] = 1.0
+    keep[roots] = 0.0
+    Pat = _csr(sp.diags(keep) @ Pat)  # rows that may change
+    Pat.data[:] = 1.0
+    bc = Bc[:, 0]
+    wrow = np.asarray(Pat @ (bc * bc)).ravel()
+    wrow = np.where(wrow > 0, wrow, 1.0)
+    PatB = _csr(Pat @ sp.diags(bc))
+
+    def project(M):
+        M = _csr(M.multiply(Pat))
+        c = np.asarray(M @ bc).ravel() / wrow  # remove each row's component along B_c
+        return _csr(M - sp.diags(c) @ PatB)
+
+    d = A.diagonal()
+    dinv = sp.diags(np.where(d != 0, 1.0 / np.where(d != 0, d, 1.0), 0.0))
+    P = T.copy()
+    R = project(-(A @ P))
+    Z = project(dinv @ R)
+    rz = R.multiply(Z).sum()
+    Pd = Z
+    for _ in range(maxiter):
+        if not np.isfinite(rz) or rz <= 0:
+            break
+        AP = A @ Pd
+        pap = Pd.multiply(AP).sum()
+        if pap <= 0:
+            break
+        alpha = rz / pap
+        P = _csr(P + alpha * Pd)
+        R = _csr(R - alpha * project(AP))
+        Z = project(dinv @ R)
+        rz_new = R.multiply(Z).sum()
+        Pd = _csr(Z + (rz_new / rz) * Pd)
+        rz = rz_new
+    P.eliminate_zeros()
+    return _csr(P)
+
+
+def rootnode_solver(A, B=None, max_levels=10, max_coarse=10, theta=0.0, improve_iterations=4, degree=2,
+                    maxiter=4, **_ignored):
+    """Build a root-node hierarchy with the defaults listed in the module docstring."""
+    A = _csr(A).astype(np.float64)
+    B = np.ones((A.shape[0], 1)) if B is None else np.asarray(B, dtype=np.float64).reshape(A.shape[0], -1)
+    levels = [HostLevel(A)]
+    while len(levels) < max_levels and levels[-1].A.shape[0] > max_coarse:
+        A = levels[-1].A
+        S = _symmetric_strength(A, theta)
+        agg, nagg, roots = _standard_aggregation(S, return_roots=True)
+        if nagg == 0 or nagg >= A.shape[0]:
+            break
+        if len(levels) == 1 and improve_iterations:
+            B = _symmetric_gauss_seidel(A, B[:, 0].copy(), np.zeros(A.shape[0]), improve_iterations).reshape(-1, 1)
+        T, Bc = _rootnode_tentative(agg, nagg, roots, B)
+        P = _energy_prolongation(A, T, Bc, roots, np.nonzero(agg >= 0)[0], degree, maxiter)
+        R = _csr(P.T)
+        levels[-1].P = P
+        levels[-1].R = R
+        levels.append(HostLevel(_csr(R @ A @ P)))
+        B = Bc
+    return HostHierarchy(levels, kind="rootnode")
+
+
+# ---------------------------------------------------------------- pairwise
+
+def _pairwise_pass(A, beta=0.25, dd_factor=5.0):
+    """One pairing pass (Notay 2010, Algorithm 4.1 with natural node order): every free node
+    i is paired with the free j != i of most negative a_ij among its strong negative
+    couplings (a_ij < -beta max_k |a_ik|), or left alone when it has none.  Rows with
+    a_ii > dd_factor * sum_{j != i} |a_ij| are left out of the coarse grid.  Returns the
+    aggregate index per node (-1: left out) and the number of aggregates."""
+    n = A.shape[0]
+    A = _csr(A)
+    ptr, idx, val = A.indptr, A.indices, A.data
+    diag = A.diagonal()
+    offsum = np.asarray(abs(A).sum(axis=1)).ravel() - np.abs(diag)
+    agg = np.full(n, -2, dtype=np.int64)
+    agg[diag > dd_factor * offsum] = -1
+    nagg = 0
+    for i in range(n):
+        if agg[i] != -2:
+            continue
+        s, e = ptr[i], ptr[i + 1]
+        cols, vals = idx[s:e], val[s:e]
+        off = cols != i
+        cols, vals = cols[off], vals[off]
+        best = -1
+        if len(cols):
+            bound = -beta * np.max(np.abs(vals))
+            cand = (vals < bound) & (agg[cols] == -2)
+            if np.any(cand):
+                cc, cv = cols[cand], vals[cand]
+                best = int(cc[np.lexsort((cc, cv))[0]])  # most negative, ties by column
+        agg[i] = nagg
+        if best >= 0:
+            agg[best] = nagg
+        nagg += 1
+    return agg, nagg
+
+
+def _piecewise_constant(agg, nagg):
+    member = agg >= 0
+    rows = np.nonzero(member)[0]
+    return _csr(sp.csr_matrix((np.ones(len(rows)), (rows, agg[member])), shape=(len(agg), nagg)))
+
+
+def pairwise_solver(A, max_levels=10, max_coarse=10, beta=0.25, matchings=2, **_ignored):
+    """Build a pairwise-aggregation hierarchy with the defaults in the module docstring."""
+    A = _csr(A).astype(np.float64)
+    levels = [HostLevel(A)]
+    while len(levels) < max_levels and levels[-1].A.shape[0] > max_coarse:
+        A = levels[-1].A
+        P = None
+        Ak = A
+        for _ in range(matchings):
+            agg, nagg = _pairwise_pass(Ak, beta)
+            Pk = _piecewise_constant(agg, nagg)
+            P = Pk if P is None else _csr(P @ Pk)
+            Ak = _csr(Pk.T @ Ak @ Pk)
+            if nagg <= max_coarse:
+                break
+        if P.shape[1] == 0 or P.shape[1] >= A.shape[0]:
+            break
+        R = _csr(P.T)
+        levels[-1].P = P
+        levels[-1].R = R
+        levels.append(HostLevel(_csr(R @ A @ P)))
+    return HostHierarchy(levels, kind="pairwise")
 
 
 # ---------------------------------------------------------------- Ruge-Stueben

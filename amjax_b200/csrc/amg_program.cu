@@ -65,7 +65,7 @@ long long spin_limit() {
 bool programs_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("AMG_PROGRAM");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
   }();
   return on;
 }

@@ -15,6 +15,10 @@ def host_hierarchy(kind: str, n: int, dim: int = 2):
         return amg_setup.smoothed_aggregation_solver(A)
     if kind == "rs":
         return amg_setup.ruge_stuben_solver(A)
+    if kind == "rootnode":
+        return amg_setup.rootnode_solver(A)
+    if kind == "pairwise":
+        return amg_setup.pairwise_solver(A)
     raise ValueError(kind)
 
 

@@ -118,7 +118,8 @@ def test_unknown_coarse_solver_raises():
 
 def test_hierarchy_builders_and_npz_roundtrip(tmp_path):
     A = gallery.poisson((30, 30))
-    for factory in (amg_setup.smoothed_aggregation_solver, amg_setup.ruge_stuben_solver):
+    for factory in (amg_setup.smoothed_aggregation_solver, amg_setup.ruge_stuben_solver,
+                    amg_setup.rootnode_solver, amg_setup.pairwise_solver):
         h = factory(A)
         assert len(h.levels) > 1 and h.levels[-1].A.shape[0] <= 10 + 60
         for i, lvl in enumerate(h.levels[:-1]):
@@ -174,3 +175,49 @@ def test_spectral_radius_on_device_needs_a_cuda_matrix():
     A = sp_.diags([2.0, 2.0, 2.0]).tocsr()
     with pytest.raises(ValueError):
         approximate_spectral_radius(A, np.full(3, 0.5), on_device=True)
+
+
+def test_rootnode_prolongation_keeps_its_constraints():
+    """Root-node AMG (Manteuffel, Olson, Schroder & Southworth 2017): P injects at the root
+    nodes, reproduces the candidate (P B_c = B on aggregated rows), and the energy
+    minimisation lowers trace(P^T A P) below the tentative prolongator's."""
+    import scipy.sparse as sp
+    A = gallery.poisson((24, 24))
+    S = amg_setup._symmetric_strength(amg_setup._csr(A))
+    agg, nagg, roots = amg_setup._standard_aggregation(S, return_roots=True)
+    B = np.ones((A.shape[0], 1))
+    T, Bc = amg_setup._rootnode_tentative(agg, nagg, roots, B)
+    P = amg_setup._energy_prolongation(amg_setup._csr(A), T, Bc, roots, np.nonzero(agg >= 0)[0])
+    np.testing.assert_allclose(P[roots].toarray(), np.eye(nagg), atol=1e-14)
+    np.testing.assert_allclose(P @ Bc[:, 0], B[:, 0], atol=1e-12)
+    energy = lambda M: float((M.T @ (A @ M)).diagonal().sum())
+    assert energy(P) < 0.9 * energy(T)
+    assert np.all(np.isin(agg[roots], np.arange(nagg))) and len(set(roots.tolist())) == nagg
+
+
+def test_pairwise_aggregates_hold_at_most_four_nodes():
+    """Double pairwise aggregation (Notay 2010): unsmoothed piecewise-constant P, each
+    aggregate (column) holds 1-4 fine nodes, each fine row at most one entry."""
+    A = gallery.poisson((32, 32))
+    h = amg_setup.pairwise_solver(A)
+    P = h.levels[0].P
+    assert set(np.unique(P.data).tolist()) == {1.0}
+    assert np.diff(P.indptr).max() <= 1
+    sizes = np.asarray(P.sum(axis=0)).ravel()
+    assert sizes.min() >= 1 and sizes.max() <= 4
+    assert P.shape[1] < A.shape[0] / 3
+
+
+@pytest.mark.parametrize("factory", ["rootnode_solver", "pairwise_solver"])
+def test_new_factories_converge_in_the_oracle(factory):
+    """The hierarchies drive the FP64 oracle's V-cycle PCG and standalone solve to 1e-8."""
+    from oracle import amg_oracle as O
+    A = gallery.poisson((40, 40))
+    h = getattr(amg_setup, factory)(A)
+    W = ("jacobi", {"iterations": 1, "omega": 2.0 / 3.0})
+    oml = O.Hierarchy.from_host(h, presmoother=W, postsmoother=W)
+    b = np.random.default_rng(0).standard_normal(A.shape[0])
+    x, k = O.cg(A, b, tol=1e-8, maxiter=200, M=O.aspreconditioner(oml))
+    assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b) and k < 60
+    x, it, rr = O.solve_loop(oml, b, tol=1e-8, maxiter=400)
+    assert rr < 1e-8

@@ -229,9 +229,10 @@ def test_air_convection_diffusion_gradients():
     np.testing.assert_allclose(float(gv.cpu().numpy() @ dv), fd_v, rtol=1e-6)
 
 
-@pytest.mark.parametrize("factory", ["smoothed_aggregation_solver", "ruge_stuben_solver", "air_solver"])
+@pytest.mark.parametrize("factory", ["smoothed_aggregation_solver", "rootnode_solver", "pairwise_solver",
+                                     "ruge_stuben_solver", "air_solver"])
 def test_from_pyamg_compatibility(factory):
-    """tests/test_multilevel.py:322-333 for the factories restated here."""
+    """tests/test_multilevel.py:322-333: all five factories the reference lists."""
     A = gallery.poisson((20, 20))
     assert len(MultilevelSolver.from_pyamg(getattr(amg_setup, factory)(A), coarse_solver="jacobi").levels) > 1
     ml = MultilevelSolver.from_pyamg(getattr(amg_setup, factory)(A), presmoother=RHO, postsmoother=RHO,

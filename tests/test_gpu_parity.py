@@ -87,7 +87,7 @@ def test_inverse_diagonal_zero_rule():
 
 
 # ------------------------------------------------------------------ standalone solve parity
-@pytest.mark.parametrize("kind", ["rs", "sa"])
+@pytest.mark.parametrize("kind", ["rs", "sa", "rootnode", "pairwise"])
 @pytest.mark.parametrize("cycle", ["V", "W", "F"])
 def test_solve_per_iterate_fp64(kind, cycle):
     """FP64 iterates equal the oracle's per cycle to <= 1e-10 relative."""

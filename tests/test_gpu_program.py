@@ -1,8 +1,8 @@
 """GPU tests of the persistent coarse-level program (one cooperative launch that runs a
 cycle's coarse levels with grid barriers between dependent steps).
 
-* The program path gives bit-identical solutions and identical iteration counts to the
-  launch-per-step path (AMG_PROGRAM=0) for the standalone solve and PCG, V / W / F cycles
+* The program path (AMG_PROGRAM=1) gives bit-identical solutions and identical iteration
+  counts to the launch-per-step path for the standalone solve and PCG, V / W / F cycles
   (W and F record more steps than one launch holds, so several programs run in a row),
   k = 1 and k > 1, FP64, FP32 and mixed precision: its row loops keep the launched
   kernels' multiply-add order.
@@ -11,7 +11,8 @@ cycle's coarse levels with grid barriers between dependent steps).
   context stays usable (a plain FP64 SpMV runs afterwards).
 
 Each configuration runs in a child process because the switches are read once per
-process.
+process; the two runs of a comparison share one tuning file, so both launch the same lane
+layouts (with k = 1 the lanes that split a row's nonzeros set its summation order).
 """
 
 import json
@@ -61,10 +62,11 @@ def _run(env_extra, script):
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
-def test_program_path_is_bit_identical_to_launches():
+def test_program_path_is_bit_identical_to_launches(tmp_path):
     script = SCRIPT.format(root=ROOT)
-    with_prog = _run({}, script)
-    without = _run({"AMG_PROGRAM": "0"}, script)
+    tune = str(tmp_path / "tune.txt")
+    with_prog = _run({"AMG_PROGRAM": "1", "AMG_TUNE_FILE": tune}, script)
+    without = _run({"AMG_PROGRAM": "0", "AMG_TUNE_FILE": tune}, script)
     fewer = with_prog.pop("launches")
     more = without.pop("launches")
     assert set(with_prog) == set(without)
@@ -103,7 +105,7 @@ print(json.dumps(res))
 
 
 def test_barrier_timeout_is_reported_not_hung():
-    res = _run({"AMG_SPIN_LIMIT": "16"}, TIMEOUT_SCRIPT.format(root=ROOT))
+    res = _run({"AMG_PROGRAM": "1", "AMG_SPIN_LIMIT": "16"}, TIMEOUT_SCRIPT.format(root=ROOT))
     assert res["solve"] == 4 and res["pcg"] == 4, res
     assert "ran out of time" in res["pcg_msg"]
     assert res["spmv_ok"]
