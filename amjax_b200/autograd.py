@@ -6,10 +6,14 @@ with the same kernels on the transposed hierarchy (the reference solves ``A lamb
 correct only for symmetric A; for a symmetric hierarchy the two coincide and the
 hierarchy is reused).  Then ``dL/db = lambda`` and ``dL/dA_ij = -sum_c lambda_ic x_jc``:
 for a sparse operator (``SparseA``) sampled on A's stored pattern by the library's
-kernel, for a dense tensor A the dense ``-lambda x^T`` the reference returns.
+kernel, for a dense tensor A the dense ``-lambda x^T`` the reference returns.  In FP64
+and the mixed precisions the backward solve and the sampled product are one library call
+(``amg_adjoint``, the entry point an XLA/JAX binding of the custom VJP would call).
 """
 
 from __future__ import annotations
+
+import ctypes as C
 
 import numpy as np
 import scipy.sparse as sp
@@ -83,11 +87,17 @@ class _SolveFn(torch.autograd.Function):
         ml, opts, a_obj = ctx.ml, ctx.opts, ctx.a_obj
         mlt = ml.transposed()
         At = _transposed_operator(ml, a_obj)
-        lam = _run(mlt, opts, gx.contiguous(), At)
+        want_values = isinstance(a_obj, SparseA) and a_obj.values.requires_grad
         grad_a = None
-        if isinstance(a_obj, SparseA) and a_obj.values.requires_grad:
-            grad_a = sampled_outer(a_obj.pattern, lam, x).to(a_obj.values.dtype)
-        elif isinstance(a_obj, torch.Tensor) and a_obj.requires_grad:
+        if ml._precision(opts["precision"]) != N.PREC_F32:  # one library call: A^-T solve + sampled product
+            lam, gv = adjoint(mlt, opts, gx, x, At, a_obj.pattern if want_values else None)
+            if want_values:
+                grad_a = gv.to(a_obj.values.dtype)
+        else:
+            lam = _run(mlt, opts, gx.contiguous(), At)
+            if want_values:
+                grad_a = sampled_outer(a_obj.pattern, lam, x).to(a_obj.values.dtype)
+        if isinstance(a_obj, torch.Tensor) and a_obj.requires_grad:
             lam2 = lam.reshape(lam.shape[0], -1)
             x2 = x.reshape(x.shape[0], -1)
             grad_a = (-(lam2 @ x2.T)).to(a_obj.dtype).to(a_obj.device)
@@ -123,6 +133,32 @@ def _run(ml, opts, bd, A0):
     else:
         x, _ = ml._solve_dev(bd, A0, opts["tol"], opts["maxiter"], opts["cycle"], opts["cycles_per_level"], prec)
     return x
+
+
+def adjoint(mlt, opts, gx, x, At=None, pattern=None):
+    """The backward solve and the values gradient in one library call (``amg_adjoint``):
+    ``lam = A^-T gx`` on the transposed hierarchy ``mlt`` (standalone cycles or PCG as
+    ``opts["method"]`` says, the forward solve's tolerance, cycle and precision), and with
+    ``pattern`` (A's CSR pattern) ``grad[e] = -sum_c lam[row(e), c] x[col(e), c]``.
+    Returns ``(lam, grad or None)``; FP64 throughout."""
+    dev = mlt.levels[0].A.device
+    g = gx.detach().to(device=dev, dtype=torch.float64).contiguous()
+    k = 1 if g.dim() == 1 else int(g.shape[1])
+    lam = torch.empty_like(g)
+    maxiter = opts["maxiter"] if opts["maxiter"] is not None else 10 * int(g.shape[0])
+    grad = xd = None
+    if pattern is not None:
+        grad = torch.empty(pattern.nnz, dtype=torch.float64, device=dev)
+        xd = x.detach().to(device=dev, dtype=torch.float64).contiguous()
+    iters = (C.c_int32 * k)()
+    rel = (C.c_double * k)()
+    N.call("amg_adjoint", mlt._native(), mlt._precision(opts["precision"]), 1 if opts["method"] == "pcg" else 0,
+           N.ptr(g), N.ptr(xd), k, float(opts["tol"]), float(opts["atol"]), int(maxiter), N.CYCLES[opts["cycle"]],
+           int(opts["cycles_per_level"]), C.byref(At.desc()) if At is not None else None,
+           C.byref(pattern.desc()) if pattern is not None else None, N.ptr(lam), N.ptr(grad), iters, rel,
+           N.stream_ptr())
+    mlt.last_info = {"iterations": list(iters), "relres": list(rel)}
+    return lam, grad
 
 
 def sampled_outer(pattern: CSRMatrix, lam: torch.Tensor, x: torch.Tensor) -> torch.Tensor:

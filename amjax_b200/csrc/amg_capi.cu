@@ -73,6 +73,59 @@ static void jacobi_impl(const amg_csr* Ad, const void* x, const void* b, const v
 }
 
 
+// Bodies of amg_solve / amg_pcg (also run by amg_adjoint).
+static void solve_body(amg_hierarchy* h, int precision, const void* b, void* x, int k, double tol, int maxiter,
+                       int cycle, int cycles_per_level, const amg_csr* A0, int32_t* iters_out, double* relres_out,
+                       cudaStream_t s) {
+  if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
+  check_vec(b, "b");
+  check_vec(x, "x");
+  if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
+  if (maxiter < 0) fail(AMG_ERR_INVALID_ARG, "maxiter must be >= 0");
+  cycle_char(cycle);
+  std::lock_guard<std::mutex> lk(h->mu);
+  Csr a0;
+  const Csr* pa0 = nullptr;
+  if (A0) { a0 = override_csr(h, A0, s); pa0 = &a0; }
+  check_prec_data(h, precision, pa0);
+  Plan* pl = get_plan(h, precision, k, s);
+  Req q{precision, k, cycle, cycles_per_level, maxiter, tol, 0.0, b, x, pa0};
+  q.program = true;
+  if (precision == AMG_PREC_F64) solve_plain<double>(h, pl, q, s);
+  else if (precision == AMG_PREC_F32) solve_plain<float>(h, pl, q, s);
+  else if (is_mixed(precision)) solve_mixed(h, pl, q, s);
+  else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
+  read_results(pl, s, false, iters_out, relres_out);
+}
+
+static void pcg_body(amg_hierarchy* h, int precision, const void* b, void* x, int k, double tol, double atol,
+                     int maxiter, int cycle, int cycles_per_level, const amg_csr* A0, int32_t* iters_out,
+                     double* relres_out, cudaStream_t s) {
+  if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
+  check_vec(b, "b");
+  check_vec(x, "x");
+  if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
+  if (maxiter < 0) fail(AMG_ERR_INVALID_ARG, "maxiter must be >= 0");
+  cycle_char(cycle);
+  std::lock_guard<std::mutex> lk(h->mu);
+  Csr a0;
+  const Csr* pa0 = nullptr;
+  if (A0) { a0 = override_csr(h, A0, s); pa0 = &a0; }
+  check_prec_data(h, precision, nullptr);
+  if (pa0 && (precision == AMG_PREC_F32 ? !pa0->v32 : !pa0->v64))
+    fail(AMG_ERR_INVALID_ARG, "A0 lacks values for this precision");
+  Plan* pl = get_plan(h, precision, k, s);
+  Req q{precision, k, cycle, cycles_per_level, maxiter, tol, atol, b, x, pa0};
+  q.program = true;
+  if (precision == AMG_PREC_F64) pcg<double, double>(h, pl, q, s);
+  else if (precision == AMG_PREC_F32) pcg<float, float>(h, pl, q, s);
+  else if (precision == AMG_PREC_MIXED && (!pa0 || pa0->v32)) pcg_ru(h, pl, q, s);
+  else if (is_mixed(precision)) pcg<double, float>(h, pl, q, s);
+  else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
+  read_results(pl, s, true, iters_out, relres_out);
+}
+
+
 extern "C" {
 
 amg_status amg_hierarchy_create(const amg_level_desc* levels, int32_t n_levels,
@@ -144,26 +197,8 @@ amg_status amg_solve(amg_hierarchy* h, int32_t precision, const void* b, void* x
                      double tol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
                      const amg_csr* A0, int32_t* iters_out, double* relres_out, void* stream) {
   return guarded([&] {
-    if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
-    check_vec(b, "b");
-    check_vec(x, "x");
-    if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
-    if (maxiter < 0) fail(AMG_ERR_INVALID_ARG, "maxiter must be >= 0");
-    cycle_char(cycle);
-    std::lock_guard<std::mutex> lk(h->mu);
-    Csr a0;
-    const Csr* pa0 = nullptr;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (A0) { a0 = override_csr(h, A0, s); pa0 = &a0; }
-    check_prec_data(h, precision, pa0);
-    Plan* pl = get_plan(h, precision, k, s);
-    Req q{precision, k, cycle, cycles_per_level, maxiter, tol, 0.0, b, x, pa0};
-    q.program = true;
-    if (precision == AMG_PREC_F64) solve_plain<double>(h, pl, q, s);
-    else if (precision == AMG_PREC_F32) solve_plain<float>(h, pl, q, s);
-    else if (is_mixed(precision)) solve_mixed(h, pl, q, s);
-    else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
-    read_results(pl, s, false, iters_out, relres_out);
+    solve_body(h, precision, b, x, k, tol, maxiter, cycle, cycles_per_level, A0, iters_out, relres_out,
+               static_cast<cudaStream_t>(stream));
   });
 }
 
@@ -192,29 +227,41 @@ amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, 
                    int32_t cycles_per_level, const amg_csr* A0, int32_t* iters_out,
                    double* relres_out, void* stream) {
   return guarded([&] {
-    if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
-    check_vec(b, "b");
-    check_vec(x, "x");
-    if (k < 1) fail(AMG_ERR_INVALID_ARG, "k must be >= 1");
-    if (maxiter < 0) fail(AMG_ERR_INVALID_ARG, "maxiter must be >= 0");
-    cycle_char(cycle);
-    std::lock_guard<std::mutex> lk(h->mu);
-    Csr a0;
-    const Csr* pa0 = nullptr;
+    pcg_body(h, precision, b, x, k, tol, atol, maxiter, cycle, cycles_per_level, A0, iters_out, relres_out,
+             static_cast<cudaStream_t>(stream));
+  });
+}
+
+amg_status amg_adjoint(amg_hierarchy* ht, int32_t precision, int32_t method, const void* gx, const double* x,
+                       int32_t k, double tol, double atol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
+                       const amg_csr* At, const amg_csr* pattern, void* lam, double* grad, int32_t* iters_out,
+                       double* relres_out, void* stream) {
+  return guarded([&] {
+    if (precision == AMG_PREC_F32)
+      fail(AMG_ERR_UNSUPPORTED, "amg_adjoint returns FP64 gradients: use F64, MIXED or MIXED_F64CG");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (A0) { a0 = override_csr(h, A0, s); pa0 = &a0; }
-    check_prec_data(h, precision, nullptr);
-    if (pa0 && (precision == AMG_PREC_F32 ? !pa0->v32 : !pa0->v64))
-      fail(AMG_ERR_INVALID_ARG, "A0 lacks values for this precision");
-    Plan* pl = get_plan(h, precision, k, s);
-    Req q{precision, k, cycle, cycles_per_level, maxiter, tol, atol, b, x, pa0};
-    q.program = true;
-    if (precision == AMG_PREC_F64) pcg<double, double>(h, pl, q, s);
-    else if (precision == AMG_PREC_F32) pcg<float, float>(h, pl, q, s);
-    else if (precision == AMG_PREC_MIXED && (!pa0 || pa0->v32)) pcg_ru(h, pl, q, s);
-    else if (is_mixed(precision)) pcg<double, float>(h, pl, q, s);
-    else fail(AMG_ERR_INVALID_ARG, "unknown precision %d", precision);
-    read_results(pl, s, true, iters_out, relres_out);
+    if (grad) {  // check the gradient's inputs before any solve runs
+      if (!pattern) fail(AMG_ERR_INVALID_ARG, "grad needs A's pattern");
+      check_vec(x, "x");
+      if (!ht) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
+      const int n0 = ht->levels[0].A.n_rows;
+      if (pattern->n_rows != n0 || pattern->n_cols != n0)
+        fail(AMG_ERR_INVALID_ARG, "pattern is %dx%d, expected %dx%d", pattern->n_rows, pattern->n_cols, n0, n0);
+      validate_csr(*pattern, "pattern", 0, s, true);
+    }
+    if (method == 0) {
+      solve_body(ht, precision, gx, lam, k, tol, maxiter, cycle, cycles_per_level, At, iters_out, relres_out, s);
+    } else if (method == 1) {
+      pcg_body(ht, precision, gx, lam, k, tol, atol, maxiter, cycle, cycles_per_level, At, iters_out, relres_out, s);
+    } else {
+      fail(AMG_ERR_INVALID_ARG, "method must be 0 (standalone solve) or 1 (PCG)");
+    }
+    if (grad && pattern->n_rows > 0) {
+      const int grid = std::max(1, std::min((pattern->n_rows + 7) / 8, dev_info().max_ctas));
+      sampled_outer_kernel<<<grid, 256, 0, s>>>(pattern->rowptr, pattern->col, pattern->n_rows,
+                                               static_cast<const double*>(lam), x, k, grad);
+      CK_LAUNCH();
+    }
   });
 }
 

@@ -155,6 +155,22 @@ amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, 
                    int32_t cycles_per_level, const amg_csr* A0, int32_t* iters_out,
                    double* relres_out, void* stream);
 
+/* Adjoint of a solve in one call: the backward pass of the custom VJP of
+ * MultilevelSolver.solve (_solve_bwd, amjax/multilevel.py:428-444).  Solves
+ * A^T lam = gx (method 0: standalone cycles as amg_solve; 1: PCG as amg_pcg) on the
+ * hierarchy `ht`, which must be built for A^T (the same handle when A and its hierarchy
+ * are symmetric, R = P^T; explicit transposed levels otherwise, e.g. for AIR), with At
+ * (nullable) overriding its level-0 operator as amg_solve's A0 does.  lam = dL/db [n, k].
+ * When grad is not NULL, also writes dL/dA on A's pattern (`pattern`, n x n; values not
+ * read): grad[e] = -sum_c lam[row(e), c] * x[col(e), c], with x [n, k] the forward
+ * solution (FP64) -- the reference's dense -outer(lam, x) (:438-442) sampled where A has
+ * entries, as amg_sampled_outer does.  gx, lam FP64 [n, k]; F32 is AMG_ERR_UNSUPPORTED.
+ * The adjoint solve stores nothing from the forward iterations. */
+amg_status amg_adjoint(amg_hierarchy* ht, int32_t precision, int32_t method, const void* gx, const double* x,
+                       int32_t k, double tol, double atol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
+                       const amg_csr* At, const amg_csr* pattern, void* lam, double* grad, int32_t* iters_out,
+                       double* relres_out, void* stream);
+
 /* Several independent PCG solves in one graph launch: system i uses hierarchy hs[i], its own
  * k[i] right-hand sides b[i] -> x[i] (layouts as in amg_pcg), and the shared tol / atol /
  * maxiter / cycle.  The reference solves one system per call (jax.vmap batches right-hand

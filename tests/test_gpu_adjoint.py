@@ -240,3 +240,39 @@ def test_from_pyamg_compatibility(factory):
     b = np.ones(A.shape[0])
     x = ml.solve(b, tol=1e-8, maxiter=300)
     assert np.linalg.norm(b - A @ x) < 1e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("method", ["solve", "pcg"])
+def test_adjoint_entry_point_equals_two_calls(method):
+    """amg_adjoint (the backward solve plus the sampled dL/dA in one call) gives exactly the
+    transposed-hierarchy solve followed by amg_sampled_outer, and rejects F32 and a
+    gradient request without a pattern."""
+    import ctypes as C
+    from amjax_b200 import _native as N
+    from amjax_b200.autograd import adjoint, sampled_outer
+    A = gallery.convection_diffusion_2d(24, peclet=10.0, angle=np.pi / 6) if method == "solve" else \
+        gallery.variable_diffusion_2d(24, sigma=1.0, seed=3)
+    host = amg_setup.air_solver(A) if method == "solve" else amg_setup.smoothed_aggregation_solver(A)
+    ml = MultilevelSolver.from_pyamg(host, presmoother=RHO, postsmoother=RHO)
+    mlt = ml.transposed()
+    pattern = CSRMatrix.from_scipy(A)
+    rng = np.random.default_rng(8)
+    gx = torch.as_tensor(rng.standard_normal((A.shape[0], 3))).cuda()
+    x = torch.as_tensor(rng.standard_normal((A.shape[0], 3))).cuda()
+    opts = dict(tol=1e-10, atol=0.0, maxiter=400, cycle="V", cycles_per_level=1, precision=None, method=method)
+    lam, grad = adjoint(mlt, opts, gx, x, None, pattern)
+    f = mlt.pcg if method == "pcg" else mlt.solve
+    lam2 = f(gx, tol=1e-10, maxiter=400)
+    assert torch.equal(lam, lam2)
+    assert torch.equal(grad, sampled_outer(pattern, lam2, x))
+    lib = N.load()
+    iters = (C.c_int32 * 3)()
+    rel = (C.c_double * 3)()
+    out = torch.empty_like(gx)
+    g = torch.empty(pattern.nnz, dtype=torch.float64, device="cuda")
+    st = lib.amg_adjoint(mlt._native(), N.PREC_F32, 0, N.ptr(gx), N.ptr(x), 3, 1e-8, 0.0, 10, 0, 1, None,
+                         C.byref(pattern.desc()), N.ptr(out), N.ptr(g), iters, rel, N.stream_ptr())
+    assert st == 2
+    st = lib.amg_adjoint(mlt._native(), N.PREC_F64, 0, N.ptr(gx), N.ptr(x), 3, 1e-8, 0.0, 10, 0, 1, None, None,
+                         N.ptr(out), N.ptr(g), iters, rel, N.stream_ptr())
+    assert st == 1
