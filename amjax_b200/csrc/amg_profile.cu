@@ -10,29 +10,34 @@ namespace {
 
 double mpass(const Csr& M, int s) { return double(M.nnz) * (s + 4) + 4.0 * (M.n_rows + 1); }
 
-// Mean device time (microseconds) of `reps` launches, each bracketed by its own events on
-// stream s and preceded (outside the events) by a write of `flush_bytes` that evicts L2.
+// Mean device time (microseconds) per launch of `reps` launches issued back to back between
+// two CUDA events on stream s, as in a solve (programmatic dependent launch overlaps each
+// launch with its predecessor's tail).  Consecutive launches alternate between two
+// disjoint buffer sets (launch(set, stream)), so each launch finds its operands evicted
+// from L2 by the other set's launch and streams them from DRAM.
 template <class F>
-double time_op(F&& launch, int reps, cudaStream_t s, void* flush, size_t flush_bytes) {
+double time_op(F&& launch, int reps, cudaStream_t s) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  launch(s);  // warm-up
-  double tot = 0.0;
-  for (int r = 0; r < reps; ++r) {
-    CK(cudaMemsetAsync(flush, r & 1, flush_bytes, s));
-    CK(cudaEventRecord(e0, s));
-    launch(s);
-    CK(cudaEventRecord(e1, s));
-    CK(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, e0, e1));
-    tot += ms;
-  }
+  launch(0, s);  // warm-up
+  launch(1, s);
+  CK(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; ++r) launch(r & 1, s);
+  CK(cudaEventRecord(e1, s));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  return tot / reps * 1e3;
+  return double(ms) / reps * 1e3;
 }
+
+// One buffer set: the fine level's vectors [n, k] and the coarse level-1 ones [nc, k].
+struct Bufs {
+  float *z, *rs, *w1, *w2, *xs, *pa, *pb, *bc, *xc;
+  double *x64, *b64;
+};
 
 }  // namespace
 
@@ -51,111 +56,129 @@ extern "C" amg_status amg_time_pcg_ops(amg_hierarchy* h, int32_t k, int32_t reps
     const Csr& A = l0.A;
     const int n = A.n_rows, nc = l1.A.n_rows;
     const double N = n, Nc = nc, K = k;
-    float* z = static_cast<float*>(pl->X[0]);
-    float* rs = static_cast<float*>(pl->B[0]);
-    float* w1 = static_cast<float*>(pl->W1[0]);
-    float* w2 = static_cast<float*>(pl->W2[0]);
-    float* xs = static_cast<float*>(pl->r_out);
-    float* pa = static_cast<float*>(pl->p_out);
-    float* pb = static_cast<float*>(pl->q_out);
-    const size_t v32 = size_t(n) * k * 4, v64 = size_t(n) * k * 8;
-    const size_t flush_bytes = size_t(256) << 20;
-    double *x64 = nullptr, *b64 = nullptr;
-    void* flush = nullptr;
-    CK(cudaMallocAsync(reinterpret_cast<void**>(&x64), v64, s));
-    CK(cudaMallocAsync(reinterpret_cast<void**>(&b64), v64, s));
-    CK(cudaMallocAsync(&flush, flush_bytes, s));
+    const size_t v32 = size_t(n) * k * 4, v64 = size_t(n) * k * 8, c32 = size_t(nc) * k * 4;
+    std::vector<void*> owned;
+    auto dalloc = [&](size_t bytes) {
+      void* p = nullptr;
+      CK(cudaMallocAsync(&p, bytes, s));
+      owned.push_back(p);
+      CK(cudaMemsetAsync(p, 0, bytes, s));
+      return p;
+    };
     struct Row { const char* name; double bytes, us; };
     std::vector<Row> rows;
     try {
-      for (void* p : {(void*)z, (void*)rs, (void*)w1, (void*)w2, (void*)xs, (void*)pa, (void*)pb})
-        CK(cudaMemsetAsync(p, 0, v32, s));
-      CK(cudaMemsetAsync(x64, 0, v64, s));
-      CK(cudaMemsetAsync(b64, 0, v64, s));
-      for (int l = 1; l < int(h->levels.size()); ++l) {
-        const size_t vl = size_t(h->levels[l].A.n_rows) * k * 4;
-        CK(cudaMemsetAsync(pl->X[l], 0, vl, s));
-        CK(cudaMemsetAsync(pl->B[l], 0, vl, s));
+      Bufs set[2];
+      for (Bufs& b : set) {
+        b.z = static_cast<float*>(dalloc(v32)); b.rs = static_cast<float*>(dalloc(v32));
+        b.w1 = static_cast<float*>(dalloc(v32)); b.w2 = static_cast<float*>(dalloc(v32));
+        b.xs = static_cast<float*>(dalloc(v32)); b.pa = static_cast<float*>(dalloc(v32));
+        b.pb = static_cast<float*>(dalloc(v32)); b.bc = static_cast<float*>(dalloc(c32));
+        b.xc = static_cast<float*>(dalloc(c32));
+        b.x64 = static_cast<double*>(dalloc(v64)); b.b64 = static_cast<double*>(dalloc(v64));
       }
+      int* one = static_cast<int*>(dalloc(sizeof(int) * 2));  // the fold's gate, set to 1
+      const int one_h = 1;
+      CK(cudaMemcpyAsync(one, &one_h, sizeof(int), cudaMemcpyHostToDevice, s));
       std::vector<int> ones(size_t(k), 1);
-      CK(cudaMemcpyAsync(pl->active(), ones.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
-      CK(cudaStreamSynchronize(s));
+      auto all_active = [&]() {
+        CK(cudaMemcpyAsync(pl->active(), ones.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+      };
+      all_active();
       const Red red = red_of(pl);
       LoopCtl ctl = make_ctl(pl, 1 << 30);
       {
-        OpCgQDir<float, float> op{pa, z, pb, pl->beta(), k, nullptr, pl->gamma(), pl->alpha()};
-        tune_op(A, op, k, red, s, {pa, z, pb});
-        rows.push_back({"cg_direction_pAp", mpass(A, 4) + 4 * K * 3 * N,
-                        time_op([&](cudaStream_t c) { run_csr(A, op, k, red, c, {pa, z, pb}); }, reps, s, flush, flush_bytes)});
+        auto mk = [&](const Bufs& b) {
+          return OpCgQDir<float, float>{b.pa, b.z, b.pb, pl->beta(), k, nullptr, pl->gamma(), pl->alpha()};
+        };
+        tune_op(A, mk(set[0]), k, red, s, {set[0].pa, set[0].z, set[0].pb});
+        rows.push_back({"cg_direction_pAp", mpass(A, 4) + 4 * K * 3 * N, time_op([&](int i, cudaStream_t c) {
+          run_csr(A, mk(set[i]), k, red, c, {set[i].pa, set[i].z, set[i].pb}); }, reps, s)});
       }
       {
-        OpCgUpdA<float, float> op{};
-        op.x = xs; op.r = rs; op.p = pb; op.r_lo = nullptr; op.alpha = pl->alpha(); op.active = pl->active();
-        op.ld = k; op.stop = nullptr; op.ctl = ctl; op.reliable = true;
-        tune_op(A, op, k, red, s, {xs, rs, pb});
-        rows.push_back({"cg_update", mpass(A, 4) + 4 * K * 5 * N,
-                        time_op([&](cudaStream_t c) { run_csr(A, op, k, red, c, {xs, rs, pb}); }, reps, s, flush, flush_bytes)});
+        auto mk = [&](const Bufs& b) {
+          OpCgUpdA<float, float> op{};
+          op.x = b.xs; op.r = b.rs; op.p = b.pb; op.r_lo = nullptr; op.alpha = pl->alpha(); op.active = pl->active();
+          op.ld = k; op.stop = nullptr; op.ctl = ctl; op.reliable = true;
+          return op;
+        };
+        tune_op(A, mk(set[0]), k, red, s, {set[0].xs, set[0].rs, set[0].pb});
+        all_active();
+        rows.push_back({"cg_update", mpass(A, 4) + 4 * K * 5 * N, time_op([&](int i, cudaStream_t c) {
+          run_csr(A, mk(set[i]), k, red, c, {set[i].xs, set[i].rs, set[i].pb}); }, reps, s)});
       }
       const float* dv = l0.template dinv<float>();
       if (l0.post.on() && dv) {
-        OpJacobi<float, XS_PLAIN> op{};
         const float om = float(l0.post.omega);
-        op.xs = XSource<float, XS_PLAIN>{w1, rs, dv, om, k};
-        op.b = rs; op.dinv = dv; op.omega = om; op.out = w2; op.ld = k;
-        op.rdot32 = rs; op.gamma = pl->gamma(); op.beta = pl->beta();
-        tune_op(A, op, k, red, s, {w1, rs, w2, rs});
-        rows.push_back({"post_smooth_with_dot", mpass(A, 4) + 4 * K * 3 * N + 4 * N,
-                        time_op([&](cudaStream_t c) { run_csr(A, op, k, red, c, {w1, rs, w2, rs}); }, reps, s, flush, flush_bytes)});
+        auto mk = [&](const Bufs& b) {
+          OpJacobi<float, XS_PLAIN> op{};
+          op.xs = XSource<float, XS_PLAIN>{b.w1, b.rs, dv, om, k};
+          op.b = b.rs; op.dinv = dv; op.omega = om; op.out = b.w2; op.ld = k;
+          op.rdot32 = b.rs; op.gamma = pl->gamma(); op.beta = pl->beta();
+          return op;
+        };
+        tune_op(A, mk(set[0]), k, red, s, {set[0].w1, set[0].rs, set[0].w2, set[0].rs});
+        rows.push_back({"post_smooth_with_dot", mpass(A, 4) + 4 * K * 3 * N + 4 * N, time_op([&](int i, cudaStream_t c) {
+          run_csr(A, mk(set[i]), k, red, c, {set[i].w1, set[i].rs, set[i].w2, set[i].rs}); }, reps, s)});
       }
       if (l0.pre.on() && dv) {
-        OpResid<float, float, XS_JAC0, true, float, false> op{};
         const float om = float(l0.pre.omega);
-        op.xs = XSource<float, XS_JAC0>{nullptr, rs, dv, om, k};
-        op.b = rs; op.out = w2; op.out_lo = nullptr; op.ld = k;
-        tune_op(A, op, k, Red{}, s, {rs, w2});
-        rows.push_back({"residual_presmoothed", mpass(A, 4) + 4 * K * 2 * N + 4 * N,
-                        time_op([&](cudaStream_t c) { run_csr(A, op, k, Red{}, c, {rs, w2}); }, reps, s, flush, flush_bytes)});
+        auto mk = [&](const Bufs& b) {
+          OpResid<float, float, XS_JAC0, true, float, false> op{};
+          op.xs = XSource<float, XS_JAC0>{nullptr, b.rs, dv, om, k};
+          op.b = b.rs; op.out = b.w2; op.out_lo = nullptr; op.ld = k;
+          return op;
+        };
+        tune_op(A, mk(set[0]), k, Red{}, s, {set[0].rs, set[0].w2});
+        rows.push_back({"residual_presmoothed", mpass(A, 4) + 4 * K * 2 * N + 4 * N, time_op([&](int i, cudaStream_t c) {
+          run_csr(A, mk(set[i]), k, Red{}, c, {set[i].rs, set[i].w2}); }, reps, s)});
       }
       {
-        OpAxpy<float, XS_ZERO> op{};
-        float* bc = static_cast<float*>(pl->B[1]);
-        op.x = w2; op.out = bc; op.ld = k;
-        tune_op(l0.R, op, k, Red{}, s, {w2, bc});
-        rows.push_back({"restriction", mpass(l0.R, 4) + 4 * K * (N + Nc),
-                        time_op([&](cudaStream_t c) { run_csr(l0.R, op, k, Red{}, c, {w2, bc}); }, reps, s, flush, flush_bytes)});
+        auto mk = [&](const Bufs& b) {
+          OpAxpy<float, XS_ZERO> op{};
+          op.x = b.w2; op.out = b.bc; op.ld = k;
+          return op;
+        };
+        tune_op(l0.R, mk(set[0]), k, Red{}, s, {set[0].w2, set[0].bc});
+        rows.push_back({"restriction", mpass(l0.R, 4) + 4 * K * (N + Nc), time_op([&](int i, cudaStream_t c) {
+          run_csr(l0.R, mk(set[i]), k, Red{}, c, {set[i].w2, set[i].bc}); }, reps, s)});
       }
       if (l0.pre.on() && dv) {
-        OpAxpy<float, XS_JAC0> op{};
-        float* xc = static_cast<float*>(pl->X[1]);
-        op.base = XSource<float, XS_JAC0>{nullptr, rs, dv, float(l0.pre.omega), k};
-        op.x = xc; op.out = w1; op.ld = k;
-        tune_op(l0.P, op, k, Red{}, s, {rs, xc, w1});
+        const float om = float(l0.pre.omega);
+        auto mk = [&](const Bufs& b) {
+          OpAxpy<float, XS_JAC0> op{};
+          op.base = XSource<float, XS_JAC0>{nullptr, b.rs, dv, om, k};
+          op.x = b.xc; op.out = b.w1; op.ld = k;
+          return op;
+        };
+        tune_op(l0.P, mk(set[0]), k, Red{}, s, {set[0].rs, set[0].xc, set[0].w1});
         rows.push_back({"prolongation_correction", mpass(l0.P, 4) + 4 * K * (2 * N + Nc) + 4 * N,
-                        time_op([&](cudaStream_t c) { run_csr(l0.P, op, k, Red{}, c, {rs, xc, w1}); }, reps, s, flush, flush_bytes)});
+                        time_op([&](int i, cudaStream_t c) {
+                          run_csr(l0.P, mk(set[i]), k, Red{}, c, {set[i].rs, set[i].xc, set[i].w1}); }, reps, s)});
       }
       {
-        OpResid<double, double, XS_PLAIN, false, float, true> op{};
-        op.xs = XSource<double, XS_PLAIN>{x64, b64, nullptr, 1.0, k};
-        op.b = b64; op.out = nullptr; op.out_lo = rs; op.ld = k; op.stop = nullptr;
-        op.ctl = ctl; op.true_rule = true;
-        tune_op(A, op, k, red, s, {x64, b64, rs});
-        rows.push_back({"true_residual_fp64", mpass(A, 8) + K * (8 * 2 * N + 4 * N),
-                        time_op([&](cudaStream_t c) { run_csr(A, op, k, red, c, {x64, b64, rs}); }, reps, s, flush, flush_bytes)});
+        auto mk = [&](const Bufs& b) {
+          OpResid<double, double, XS_PLAIN, false, float, true> op{};
+          op.xs = XSource<double, XS_PLAIN>{b.x64, b.b64, nullptr, 1.0, k};
+          op.b = b.b64; op.out = nullptr; op.out_lo = b.rs; op.ld = k; op.stop = nullptr;
+          op.ctl = ctl; op.true_rule = true;
+          return op;
+        };
+        tune_op(A, mk(set[0]), k, red, s, {set[0].x64, set[0].b64, set[0].rs});
+        rows.push_back({"true_residual_fp64", mpass(A, 8) + K * (8 * 2 * N + 4 * N), time_op([&](int i, cudaStream_t c) {
+          run_csr(A, mk(set[i]), k, red, c, {set[i].x64, set[i].b64, set[i].rs}); }, reps, s)});
       }
       {
-        OpFold<double, float> op{x64, xs, k, pl->active()};
-        rows.push_back({"fold_increment", K * N * (8 + 4) * 2,
-                        time_op([&](cudaStream_t c) { run_elem<float>(n, op, k, red, c, {x64, xs}); }, reps, s, flush, flush_bytes)});
+        rows.push_back({"fold_increment", K * N * (8 + 4) * 2, time_op([&](int i, cudaStream_t c) {
+          OpFold<double, float> op{set[i].x64, set[i].xs, k, one};
+          run_elem<float>(n, op, k, red, c, {set[i].x64, set[i].xs}); }, reps, s)});
       }
     } catch (...) {
-      cudaFreeAsync(x64, s);
-      cudaFreeAsync(b64, s);
-      cudaFreeAsync(flush, s);
+      for (void* p : owned) cudaFreeAsync(p, s);
       throw;
     }
-    CK(cudaFreeAsync(x64, s));
-    CK(cudaFreeAsync(b64, s));
-    CK(cudaFreeAsync(flush, s));
+    for (void* p : owned) CK(cudaFreeAsync(p, s));
     CK(cudaStreamSynchronize(s));
     const int m = std::min<int>(max_ops, int(rows.size()));
     for (int i = 0; i < m; ++i) {

@@ -224,8 +224,9 @@ amg_status amg_sampled_outer(const amg_csr* A, const double* lam, const double* 
  * <p, A p> pass with the direction update, the CG update, the post-smoothing sweep with
  * the fused <r, z>, the residual of the pre-smoothed iterate, restriction, prolongation
  * with correction, the FP64 true residual and the increment fold -- with the layouts the
- * solve uses (tuned first if not yet).  Each of `reps` launches is timed alone with CUDA
- * events after a write that evicts L2.  Writes up to max_ops rows: a NUL-terminated name
+ * solve uses (tuned first if not yet).  `reps` launches per kernel run back to back between
+ * two CUDA events, alternating between two disjoint buffer sets so that each streams its
+ * operands from DRAM.  Writes up to max_ops rows: a NUL-terminated name
  * (name_len bytes per row), the mean microseconds per launch and the kernel's algorithmic
  * bytes (every operand read or written once); *n_ops = rows written.  Uses the hierarchy's
  * mixed-precision scratch for k, so it must not overlap a solve on the same hierarchy. */
