@@ -39,6 +39,7 @@ void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit*
     cy.visit(0, true, ct, cpl);
   };
   auto step = [=](cudaStream_t cs, TO* p_old, TO* p_new) {
+    NvtxRange nv("amg/cg-step");
     OpCgQDir<TO, TC> qop{p_old, z, p_new, pl->beta(), k, pl->stop(), pl->gamma(), pl->alpha()};
     run_csr(*A0, qop, k, red_of(pl), cs, {p_old, z, p_new});
     OpCgUpdA<TO, TC> up{};
@@ -134,6 +135,7 @@ void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Em
     cy.visit(0, true, ct, cpl);
   };
   auto true_residual = [=](cudaStream_t cs) {
+    NvtxRange nv("amg/true-residual");
     OpFold<double, TC> fo{x, xs, k, pl->ru()};
     run_elem<TC>(n0, fo, k, red_of(pl), cs, {x, xs});
     OpResid<double, double, XS_PLAIN, false, TC, true> tr{};
@@ -143,6 +145,7 @@ void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Em
     run_csr(*A0, tr, k, red_of(pl), cs, {x, b, rs});
   };
   auto step = [=](cudaStream_t cs, TC* p_old, TC* p_new) {
+    NvtxRange nv("amg/cg-step");
     OpCgQDir<TC, TC> qop{p_old, z, p_new, pl->beta(), k, pl->stop(), pl->gamma(), pl->alpha()};
     run_csr(*A0, qop, k, red_of(pl), cs, {p_old, z, p_new});
     OpCgUpdA<TC, TC> up{};

@@ -32,6 +32,14 @@ DevInfo dev_info() {
   return d;
 }
 
+bool nvtx_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("AMG_NVTX");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 bool pdl_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("AMG_PDL");

@@ -26,6 +26,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/amg_b200.h"
 #include "amg_device.cuh"
 #include "amg_program.cuh"
@@ -224,6 +226,31 @@ struct amg_hierarchy {
 };
 
 namespace amg {
+
+// ------------------------------------------------------------------ NVTX ranges
+// Named host ranges around each level visit of a cycle and each outer-loop stage
+// (AMG_NVTX=1; off by default).  They bracket the launches they enclose: in eager mode
+// (AMG_EXEC=eager) a profiler attributes every kernel to its level (ncu --nvtx
+// --nvtx-include "amg/L1/"); under graph capture they mark only the capture itself.
+bool nvtx_enabled();
+
+struct NvtxRange {
+  bool on;
+  explicit NvtxRange(const char* fmt, ...) : on(nvtx_enabled()) {
+    if (!on) return;
+    char buf[96];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    nvtxRangePushA(buf);
+  }
+  ~NvtxRange() {
+    if (on) nvtxRangePop();
+  }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ------------------------------------------------------------------ launch helpers
 struct Cfg {
@@ -936,6 +963,7 @@ struct Cycle {
   // One visit of level l (multilevel.py:316-337).  x_zero: the incoming iterate is 0.
   // On return the new iterate is in Xb(l).
   void visit(int l, bool x_zero, char ct, int cpl) {
+    NvtxRange nv("amg/L%d/%c", l, ct);
     if (!rec && l > 0 && l == tail_from) {  // this level and all below: one persistent program
       std::vector<PStep> steps;
       rec = &steps;

@@ -11,8 +11,10 @@ cycle's coarse levels with grid barriers between dependent steps).
   context stays usable (a plain FP64 SpMV runs afterwards).
 
 Each configuration runs in a child process because the switches are read once per
-process; the two runs of a comparison share one tuning file, so both launch the same lane
-layouts (with k = 1 the lanes that split a row's nonzeros set its summation order).
+process; the two runs of a comparison read one tuning file that a first run has completed,
+so both launch the same lane layouts (with k = 1 the lanes that split a row's nonzeros set
+its summation order, and a process that tunes as it goes can meet an op before its
+reducing variant is tuned).
 """
 
 import json
@@ -65,6 +67,7 @@ def _run(env_extra, script):
 def test_program_path_is_bit_identical_to_launches(tmp_path):
     script = SCRIPT.format(root=ROOT)
     tune = str(tmp_path / "tune.txt")
+    _run({"AMG_PROGRAM": "0", "AMG_TUNE_FILE": tune}, script)  # records every layout decision
     with_prog = _run({"AMG_PROGRAM": "1", "AMG_TUNE_FILE": tune}, script)
     without = _run({"AMG_PROGRAM": "0", "AMG_TUNE_FILE": tune}, script)
     fewer = with_prog.pop("launches")
