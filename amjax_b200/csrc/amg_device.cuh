@@ -554,6 +554,125 @@ csr_kr(const int* __restrict__ rowptr, const int* __restrict__ col,
   if (RED || op.reduces()) block_reduce_k<Op, G, KV, 1>(op, rc, red);
 }
 
+// csr_kp: the lean kernel with one row per lane group (the wide 32-byte layout), its row
+// metadata software-pipelined.  Per row, csr_kr waits on a chain of loads: row pointers,
+// then the first (col, val), then its gather, then the rest of the row's (col, val), then
+// their gathers -- ncu on the FP32 CG kernels at N = 250,000, k = 64 showed ~20 stall
+// cycles per issued instruction on long scoreboards with 37 % of warp slots active.  Here
+// the next row's bounds load at the top of the row and its first (col, val) once those
+// bounds are in (mid-row), and the row's remaining (col, val) for up to kPipeB nonzeros
+// issue before any gather, so a row mostly waits on its own gathers.  Same multiply-add
+// order as csr_kr (fma(a1, x1, 0), then the row's nonzeros in order): bit-identical.
+constexpr int kPipeB = 4;
+
+template <class Op, int G, int KV, bool RED, int PB = kPipeB, int MINB = kr_min_blocks<Op, KV, RED>()>
+__global__ void __launch_bounds__(kBlock, MINB)
+csr_kp(const int* __restrict__ rowptr, const int* __restrict__ col,
+       const typename Op::V* __restrict__ val, int n_rows, Op op, RedCtx rc) {
+  count_launch();
+  if (op.stopped()) return;
+  using A = typename Op::Acc;
+  const int lane = threadIdx.x % G;
+  const int grp = (blockIdx.x * kBlock + threadIdx.x) / G;
+  const int ngrp = gridDim.x * (kBlock / G);
+  const int c0 = lane * KV;
+  double red[1][KV];
+#pragma unroll
+  for (int v = 0; v < KV; ++v) red[0][v] = 0.0;
+  if (c0 < rc.k) {
+    Op lop = op;
+    if constexpr (Op::kPrepared) lop.template prepare<KV>(c0);
+    auto gather = [&](int j, A (&v)[KV]) {
+      if constexpr (Op::kPrepared) lop.template xkp<KV>(j, c0, v);
+      else op.template xk<KV>(j, c0, v);
+    };
+    auto rows = [&](auto reducing) {
+      int row = grp;
+      int s_n = 0, e_n = 0, c_n = 0;
+      A a_n = A(0);
+      if (row < n_rows) {
+        s_n = __ldg(rowptr + row);
+        e_n = __ldg(rowptr + row + 1);
+        if (s_n < e_n) {
+          c_n = __ldg(col + s_n);
+          a_n = static_cast<A>(__ldg(val + s_n));
+        }
+      }
+      for (; row < n_rows; row += ngrp) {
+        const int s = s_n, e = e_n, c1 = c_n;
+        const A a1 = a_n;
+        const int nxt = row + ngrp;
+        int s2 = 0, e2 = 0;
+        if (nxt < n_rows) {
+          s2 = __ldg(rowptr + nxt);
+          e2 = __ldg(rowptr + nxt + 1);
+        }
+        PreT<A, KV> pre;
+        op.template prek<KV>(row, c0, pre);
+        int cr[PB > 0 ? PB : 1];
+        A ar[PB > 0 ? PB : 1];
+#pragma unroll
+        for (int j = 0; j < PB; ++j) {
+          cr[j] = c1;
+          ar[j] = A(0);
+          if (s + 1 + j < e) {
+            cr[j] = __ldg(col + s + 1 + j);
+            ar[j] = static_cast<A>(__ldg(val + s + 1 + j));
+          }
+        }
+        A acc[KV];
+        {
+          A xv[KV];
+          gather(c1, xv);
+#pragma unroll
+          for (int v = 0; v < KV; ++v) acc[v] = (s < e) ? fma(a1, xv[v], A(0)) : A(0);
+        }
+        // the next row's first (col, val): its bounds have arrived by now
+        c_n = 0;
+        a_n = A(0);
+        if (s2 < e2) {
+          c_n = __ldg(col + s2);
+          a_n = static_cast<A>(__ldg(val + s2));
+        }
+#pragma unroll
+        for (int j = 0; j < PB; ++j) {
+          if (s + 1 + j < e) {
+            A xv[KV];
+            gather(cr[j], xv);
+#pragma unroll
+            for (int v = 0; v < KV; ++v) acc[v] = fma(ar[j], xv[v], acc[v]);
+          }
+        }
+        for (int nz = s + 1 + PB; nz < e; ++nz) {
+          const int cj = __ldg(col + nz);
+          const A a = static_cast<A>(__ldg(val + nz));
+          A xv[KV];
+          gather(cj, xv);
+#pragma unroll
+          for (int v = 0; v < KV; ++v) acc[v] = fma(a, xv[v], acc[v]);
+        }
+        if constexpr (decltype(reducing)::value) {
+          op.template epik<KV>(row, c0, acc, pre, red[0]);
+        } else {
+          double unused[KV];
+#pragma unroll
+          for (int v = 0; v < KV; ++v) unused[v] = 0.0;
+          op.template epik<KV>(row, c0, acc, pre, unused);
+        }
+        s_n = s2;
+        e_n = e2;
+      }
+    };
+    if constexpr (RED) {
+      rows(std::true_type{});
+    } else {
+      if (op.reduces()) rows(std::true_type{});
+      else rows(std::false_type{});
+    }
+  }
+  if (RED || op.reduces()) block_reduce_k<Op, G, KV, 1>(op, rc, red);
+}
+
 // Elementwise over [n_rows, k] with the same (group, lane, KV, NCH) mapping.
 template <class Op, int G, int KV, int NCH>
 __global__ void __launch_bounds__(kBlock, 4)

@@ -66,12 +66,15 @@ const char* tune_file_path() {
 }
 
 // A lanes-per-row code the launchers accept: k == 1: G in {1, 2, 4, 8, 16, 32}; k > 1: a
-// plain code G in {4, 8, 16, 32}, or a lean / wide code (kLeanCode / kWideCode + G) with G
+// plain code G in {4, 8, 16, 32}, or a lean / wide / pipelined code (kLeanCode / kWideCode /
+// kPipeCode + G) with G
 // in {1, 2, 4, 8, 16, 32}.  A stale or edited tuning-file line with any other value would
 // otherwise reach a launcher that maps it to a layout covering fewer columns than k.
 bool valid_layout_code(int g, int k) {
   auto lanes = [](int v) { return v == 1 || v == 2 || v == 4 || v == 8 || v == 16 || v == 32; };
   if (k == 1) return lanes(g);
+  if (g >= kPipe2Code) return pipe_lanes(g - kPipe2Code);
+  if (g >= kPipeCode) return pipe_lanes(g - kPipeCode);
   if (g >= kWideCode) return lanes(g - kWideCode);
   if (g >= kLeanCode) return lanes(g - kLeanCode);
   return g == 4 || g == 8 || g == 16 || g == 32;

@@ -257,13 +257,20 @@ struct Cfg {
   int G = 1, KV = 1, NCH = 1, grid = 1;
   bool lean = false;  // csr_kr (two rows in flight per lane group, NCH == 1)
   bool wide = false;  // csr_kr with 32-byte vectors (KV = 32 / value size)
+  bool pipe = false;  // wide, with the row metadata software-pipelined (csr_kp)
+  bool pipe2 = false; // csr_kp sized for 2 CTAs per SM
   size_t smem = 0;
 };
 
 // A tuned lanes-per-row value of kLeanCode + G selects csr_kr with G lanes; kWideCode + G
-// selects csr_kr with G lanes of 32-byte vectors.
+// selects csr_kr with G lanes of 32-byte vectors; kPipeCode + G the same layout as csr_kp,
+// kPipe2Code + G as csr_kp sized for 2 CTAs per SM (twice the registers, no spills).  The
+// pipelined kernels are built for G in {4, 8, 16}.
 constexpr int kLeanCode = 64;
 constexpr int kWideCode = 128;
+constexpr int kPipeCode = 192;
+constexpr int kPipe2Code = 256;
+inline bool pipe_lanes(int g) { return g == 4 || g == 8 || g == 16; }
 
 // Vector width of the wide kernel when every pointer is 32-byte aligned and k is a
 // multiple of it (the row stride is k), else 0.
@@ -343,16 +350,23 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     if (tune_rowptr && !tg && fallback_tag) tg = tuned_g(tune_rowptr, tune_nnz, k, int(sizeof(T)), c.KV, fallback_tag);
     if (const char* fg = std::getenv("AMG_KB_G")) {  // manual override (experiments)
       const int g = atoi(fg);
-      const int gl = g >= kWideCode ? g - kWideCode : g >= kLeanCode ? g - kLeanCode : g;
-      if (gl == 4 || gl == 8 || gl == 16 || gl == 32 || (g >= kLeanCode && (gl == 1 || gl == 2))) tg = g;
+      const int gl = g >= kPipe2Code ? g - kPipe2Code : g >= kPipeCode ? g - kPipeCode : g >= kWideCode ? g - kWideCode
+                     : g >= kLeanCode ? g - kLeanCode : g;
+      if (g >= kPipeCode ? pipe_lanes(gl)
+                         : (gl == 4 || gl == 8 || gl == 16 || gl == 32 || (g >= kLeanCode && (gl == 1 || gl == 2))))
+        tg = g;
     }
     if (!tune_rowptr && tg >= kLeanCode) tg = 0;  // elementwise passes: no lean / wide kernels
     if (tg >= kWideCode) {
-      tg -= kWideCode;
+      const bool pipe2 = tg >= kPipe2Code;
+      const bool pipe = tg >= kPipeCode;
+      tg -= pipe2 ? kPipe2Code : pipe ? kPipeCode : kWideCode;
       const int wk = wide_kv<T>(k, ptrs);
       if (wk && k / wk <= tg) {  // one 32-byte chunk per lane
         c.KV = wk;
         c.wide = true;
+        c.pipe = pipe && pipe_lanes(tg);
+        c.pipe2 = pipe2 && c.pipe;
       }
       c.lean = true;
     } else if (tg >= kLeanCode) {
@@ -373,7 +387,7 @@ static Cfg cfg_k(int n_rows, int k, int g1, std::initializer_list<const void*> p
     if (per > kMaxCh)
       fail(AMG_ERR_UNSUPPORTED, "k=%d exceeds the per-launch column limit (%d)", k, 32 * kMaxCh * c.KV);
     c.NCH = per <= 1 ? 1 : per <= 2 ? 2 : 4;
-    if (c.NCH > 1 || c.KV == 1) c.lean = c.wide = false;
+    if (c.NCH > 1 || c.KV == 1) c.lean = c.wide = c.pipe = c.pipe2 = false;
     if (c.KV == 1 && c.NCH > 1) c.G = 32;
     c.smem = sizeof(double) * std::max<size_t>(size_t(kBlock / c.G) * k, kBlock);
   }
@@ -454,6 +468,31 @@ static void launch_kr(const Csr& M, const typename Op::V* vals, const Op& op, co
   }
 }
 
+template <class Op, int G, int KV, int MINB_RED, int MINB_PLAIN>
+static void launch_kp_t(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
+                        RedCtx rc, cudaStream_t s) {
+  if constexpr (!never_reduces<Op>::value) {
+    if (op.reduces()) {
+      auto* kern = csr_kp<Op, G, KV, true, kPipeB, MINB_RED>;
+      const int grid = cap_grid(kern, c.grid, c.smem);
+      launch(kern, grid, kBlock, c.smem, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+      return;
+    }
+  }
+  if constexpr (!always_reduces<Op>::value) {
+    auto* kern = csr_kp<Op, G, KV, false, kPipeB, MINB_PLAIN>;
+    const int grid = cap_grid(kern, c.grid, 0);
+    launch(kern, grid, kBlock, 0, s, M.rowptr, M.col, vals, M.n_rows, op, rc);
+  }
+}
+
+template <class Op, int G, int KV>
+static void launch_kp(const Csr& M, const typename Op::V* vals, const Op& op, const Cfg& c,
+                      RedCtx rc, cudaStream_t s) {
+  if (c.pipe2) launch_kp_t<Op, G, KV, 2, 2>(M, vals, op, c, rc, s);
+  else launch_kp_t<Op, G, KV, kr_min_blocks<Op, KV, true>(), kr_min_blocks<Op, KV, false>()>(M, vals, op, c, rc, s);
+}
+
 // (G, NCH) pairs: any G in {4, 8, 16, 32} with NCH in {1, 2, 4} for vector widths >= 2;
 // scalar columns (odd k) use NCH = 1, or G = 32 with NCH in {2, 4}.
 template <class Op, int KV, int G>
@@ -503,6 +542,13 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
       case 8: launch_k1<Op, 8>(M, vals, op, c, rc, s); break;
       case 16: launch_k1<Op, 16>(M, vals, op, c, rc, s); break;
       default: launch_k1<Op, 32>(M, vals, op, c, rc, s); break;
+    }
+  } else if (c.wide && c.pipe) {
+    constexpr int KW = 32 / int(sizeof(typename Op::Acc));
+    switch (c.G) {
+      case 4: launch_kp<Op, 4, KW>(M, vals, op, c, rc, s); break;
+      case 8: launch_kp<Op, 8, KW>(M, vals, op, c, rc, s); break;
+      default: launch_kp<Op, 16, KW>(M, vals, op, c, rc, s); break;
     }
   } else if (c.wide) {
     constexpr int KW = 32 / int(sizeof(typename Op::Acc));
@@ -570,10 +616,15 @@ void tune_op(const Csr& M, const Op& op, int k, const Red& red, cudaStream_t s,
     for (int g = 1; g <= gmax; g <<= 1)
       if (nch <= g && (g >= 4 || kv * int(sizeof(T)) == 16 || kv * int(sizeof(T)) == 8))
         cands.push_back(kLeanCode + g);
-  if (const int wk = k > 1 ? wide_kv<T>(k, ptrs) : 0)  // the wide lean kernel, one 32-byte chunk per lane
+  if (const int wk = k > 1 ? wide_kv<T>(k, ptrs) : 0)  // the wide lean kernels, one 32-byte chunk per lane
     for (int g = 1; g <= 32; g <<= 1)
-      if (k / wk <= g && g < 2 * std::max(4, pow2ceil(k / wk)) && (g >= 4 || g == pow2ceil(k / wk)))
+      if (k / wk <= g && g < 2 * std::max(4, pow2ceil(k / wk)) && (g >= 4 || g == pow2ceil(k / wk))) {
         cands.push_back(kWideCode + g);
+        if (pipe_lanes(g)) {
+          cands.push_back(kPipeCode + g);
+          cands.push_back(kPipe2Code + g);
+        }
+      }
   if (cands.size() <= 1) {
     set_tuned_g(M.rowptr, M.nnz, k, int(sizeof(T)), kv, tag, cands.empty() ? gmax : cands[0], true);
     return;

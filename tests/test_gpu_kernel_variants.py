@@ -1,6 +1,8 @@
 """Every CSR kernel family the autotuner can pick, forced one at a time (AMG_KB_G: G lanes
 per row for csr_kb, 64 + G for the lean csr_kr, 128 + G for the wide 32-byte-vector csr_kr,
-including the 1- and 2-lane groups), so that a layout the tuner picks on some other
+192 + G for its software-pipelined form csr_kp and 256 + G for csr_kp sized for 2 CTAs
+per SM, including the 1- and 2-lane groups), so
+that a layout the tuner picks on some other
 matrix or machine is covered by a parity test here.
 
 * Jacobi sweeps through the C ABI: all families accumulate each row in nonzero order with
@@ -26,7 +28,8 @@ from amjax_b200 import _native as N
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-FAMILIES = ["16", "8", "80", "136", "65", "66", "129", "130"]  # kb 16/8, lean 16/1/2, wide 8/1/2
+FAMILIES = ["16", "8", "80", "136", "65", "66", "129", "130", "200", "196", "264", "260"]  # kb 16/8,
+# lean 16/1/2, wide 8/1/2, pipelined wide 8/4, pipelined wide at 2 CTAs per SM 8/4
 
 
 def _sweep(A, dt, x, b, dinv, omega):
@@ -84,7 +87,7 @@ print(json.dumps(out))
 
 def test_pcg_families_converge_identically():
     results = {}
-    for fam in ["16", "80", "136", "65", "130"]:
+    for fam in ["16", "80", "136", "65", "130", "200", "264"]:
         env = dict(os.environ, AMG_KB_G=fam, AMG_TUNE="0")
         r = subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT)], env=env, capture_output=True,
                            text=True, timeout=600)
