@@ -55,6 +55,9 @@ SIGNATURES = {
     "amg_pcg": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_double,
                           C.c_int32, C.c_int32, C.c_int32, C.POINTER(amg_csr), C.POINTER(C.c_int32),
                           C.POINTER(C.c_double), C.c_void_p]),
+    "amg_pcg_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_double,
+                               C.c_double, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                               C.POINTER(C.c_double), C.c_void_p]),
     "amg_adjoint": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_double,
                               C.c_double, C.c_int32, C.c_int32, C.c_int32, C.POINTER(amg_csr), C.POINTER(amg_csr),
                               C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double), C.c_void_p]),

@@ -232,6 +232,75 @@ amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, 
   });
 }
 
+amg_status amg_pcg_host(amg_hierarchy* h, int32_t precision, const double* b_host, double* x_host, int32_t k,
+                        int32_t blocks, double tol, double atol, int32_t maxiter, int32_t cycle,
+                        int32_t cycles_per_level, int32_t* iters_out, double* relres_out, void* stream) {
+  return guarded([&] {
+    if (!h) fail(AMG_ERR_INVALID_ARG, "null hierarchy");
+    if (!b_host || !x_host) fail(AMG_ERR_INVALID_ARG, "null host buffer");
+    if (precision == AMG_PREC_F32) fail(AMG_ERR_UNSUPPORTED, "amg_pcg_host moves FP64 vectors: use F64 or a mixed precision");
+    if (k < 1 || blocks < 1) fail(AMG_ERR_INVALID_ARG, "k and blocks must be >= 1");
+    std::lock_guard<std::mutex> sl(h->stage_mu);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int n = h->levels[0].A.n_rows;
+    const int kc = (k + blocks - 1) / blocks;
+    const int nb = (k + kc - 1) / kc;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    HostStage* st = h->stage.get();
+    if (!st || st->dev != dev || st->n != n || st->kc < kc) {
+      h->stage.reset();
+      auto ns = std::make_unique<HostStage>();
+      ns->dev = dev;
+      ns->n = n;
+      ns->kc = kc;
+      const size_t bytes = std::max<size_t>(size_t(n) * kc * sizeof(double), 256);
+      for (int i = 0; i < 2; ++i) {
+        CK(cudaMalloc(reinterpret_cast<void**>(&ns->b[i]), bytes));
+        CK(cudaMalloc(reinterpret_cast<void**>(&ns->x[i]), bytes));
+        CK(cudaEventCreateWithFlags(&ns->in_done[i], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ns->solved[i], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ns->out_done[i], cudaEventDisableTiming));
+      }
+      CK(cudaStreamCreateWithFlags(&ns->h2d, cudaStreamNonBlocking));
+      CK(cudaStreamCreateWithFlags(&ns->d2h, cudaStreamNonBlocking));
+      h->stage = std::move(ns);
+      st = h->stage.get();
+    }
+    // the caller's earlier work on s (e.g. writes into the host buffers' device sources)
+    // comes first
+    cudaEvent_t start;
+    CK(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    CK(cudaEventRecord(start, s));
+    CK(cudaStreamWaitEvent(st->h2d, start, 0));
+    cudaEventDestroy(start);
+    auto width = [&](int c) { return std::min(kc, k - c * kc); };
+    auto copy_in = [&](int c) {  // block c -> slot c % 2, once the solve of block c - 2 is done with it
+      const int sl2 = c & 1, w = width(c);
+      if (c >= 2) CK(cudaStreamWaitEvent(st->h2d, st->solved[sl2], 0));
+      CK(cudaMemcpy2DAsync(st->b[sl2], size_t(w) * 8, b_host + size_t(c) * kc, size_t(k) * 8, size_t(w) * 8, size_t(n),
+                           cudaMemcpyHostToDevice, st->h2d));
+      CK(cudaEventRecord(st->in_done[sl2], st->h2d));
+    };
+    copy_in(0);
+    if (nb > 1) copy_in(1);
+    for (int c = 0; c < nb; ++c) {
+      const int sl2 = c & 1, w = width(c);
+      CK(cudaStreamWaitEvent(s, st->in_done[sl2], 0));
+      if (c >= 2) CK(cudaStreamWaitEvent(s, st->out_done[sl2], 0));  // x slot drained to the host
+      pcg_body(h, precision, st->b[sl2], st->x[sl2], w, tol, atol, maxiter, cycle, cycles_per_level, nullptr,
+               iters_out ? iters_out + size_t(c) * kc : nullptr, relres_out ? relres_out + size_t(c) * kc : nullptr, s);
+      CK(cudaEventRecord(st->solved[sl2], s));
+      CK(cudaStreamWaitEvent(st->d2h, st->solved[sl2], 0));
+      CK(cudaMemcpy2DAsync(x_host + size_t(c) * kc, size_t(k) * 8, st->x[sl2], size_t(w) * 8, size_t(w) * 8, size_t(n),
+                           cudaMemcpyDeviceToHost, st->d2h));
+      CK(cudaEventRecord(st->out_done[sl2], st->d2h));
+      if (c + 2 < nb) copy_in(c + 2);
+    }
+    CK(cudaStreamSynchronize(st->d2h));
+  });
+}
+
 amg_status amg_adjoint(amg_hierarchy* ht, int32_t precision, int32_t method, const void* gx, const double* x,
                        int32_t k, double tol, double atol, int32_t maxiter, int32_t cycle, int32_t cycles_per_level,
                        const amg_csr* At, const amg_csr* pattern, void* lam, double* grad, int32_t* iters_out,

@@ -218,11 +218,36 @@ struct Plan {
 
 }  // namespace amg
 
+namespace amg {
+// Staging of amg_pcg_host: two device (B, X) column blocks [n, kc] in FP64, a copy stream
+// each way, and the events that order the copies against the block solves.
+struct HostStage {
+  int dev = -1, n = 0, kc = 0;
+  double* b[2] = {nullptr, nullptr};
+  double* x[2] = {nullptr, nullptr};
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t in_done[2] = {}, solved[2] = {}, out_done[2] = {};
+  ~HostStage() {
+    for (int i = 0; i < 2; ++i) {
+      if (b[i]) cudaFree(b[i]);
+      if (x[i]) cudaFree(x[i]);
+      if (in_done[i]) cudaEventDestroy(in_done[i]);
+      if (solved[i]) cudaEventDestroy(solved[i]);
+      if (out_done[i]) cudaEventDestroy(out_done[i]);
+    }
+    if (h2d) cudaStreamDestroy(h2d);
+    if (d2h) cudaStreamDestroy(d2h);
+  }
+};
+}  // namespace amg
+
 struct amg_hierarchy {
   std::vector<amg::Level> levels;
   amg::Coarse coarse;
   std::mutex mu;
   std::map<std::string, std::unique_ptr<amg::Plan>> plans;
+  std::mutex stage_mu;                     // one amg_pcg_host call at a time per hierarchy
+  std::unique_ptr<amg::HostStage> stage;
 };
 
 namespace amg {

@@ -310,6 +310,21 @@ def run_ours(args):
 
     # ---- headline: timed block bracketed by barrier + synchronize, max over ranks
     headline = pcg(B, prec_mixed)
+    # first call: autotuning of every op layout, graph capture and instantiation (host wall
+    # clock, synchronised); then a call on fresh B / X buffers: graphs are keyed by buffer
+    # addresses, so it captures again (tuning is cached)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    headline()
+    torch.cuda.synchronize()
+    first_call_ms = (time.perf_counter() - t0) * 1e3
+    B2 = B.clone()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ml._pcg_dev(B2, None, args.tol, 0.0, 500, "V", 1, prec_mixed)
+    torch.cuda.synchronize()
+    new_buffers_ms = (time.perf_counter() - t0) * 1e3
+    del B2
     for _ in range(args.warmup):
         headline()
     torch.cuda.synchronize()
@@ -341,6 +356,9 @@ def run_ours(args):
            "solve_bandwidth": {"bytes_per_solve_model": sbytes, "gbs": sbytes / (ms_per_step * 1e-3) / 1e9,
                                "frac_of_" + peak_kind: sbytes / (ms_per_step * 1e-3) / 1e9 / hbm_peak},
            "gpu_launches": int(launches),
+           "first_call_ms": {"cold": first_call_ms, "new_buffers": new_buffers_ms,
+                             "note": "host wall clock of the first call (autotuning + graph capture + solve) and "
+                                     "of a call on new buffers (capture + solve); steady state is value"},
            "published_reference_ms": PUBLISHED}
 
     xh = x.cpu().numpy()

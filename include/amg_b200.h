@@ -155,6 +155,20 @@ amg_status amg_pcg(amg_hierarchy* h, int32_t precision, const void* b, void* x, 
                    int32_t cycles_per_level, const amg_csr* A0, int32_t* iters_out,
                    double* relres_out, void* stream);
 
+/* amg_pcg with the right-hand sides and the solution in HOST memory (pinned, so that the
+ * copies run asynchronously): what a caller whose data lives on the host -- a CPU-side
+ * JAX array, a numpy user of MultilevelSolver.pcg -- would otherwise do as copy in, solve,
+ * copy out one after another.  b_host, x_host: [n0, k] row-major FP64 (F64, MIXED,
+ * MIXED_F64CG; F32 is AMG_ERR_UNSUPPORTED).  The k columns are solved in `blocks`
+ * contiguous column blocks (columns are independent, each with its own stop rule), and
+ * the copy of the next block in and of the previous block out overlap the current block's
+ * solve (two copy streams, strided 2D copies).  Returns when x_host holds the solution.
+ * The staging buffers (2 x 2 blocks of n0 x ceil(k / blocks) doubles) are kept with the
+ * hierarchy; calls on one hierarchy are serialised. */
+amg_status amg_pcg_host(amg_hierarchy* h, int32_t precision, const double* b_host, double* x_host, int32_t k,
+                        int32_t blocks, double tol, double atol, int32_t maxiter, int32_t cycle,
+                        int32_t cycles_per_level, int32_t* iters_out, double* relres_out, void* stream);
+
 /* Adjoint of a solve in one call: the backward pass of the custom VJP of
  * MultilevelSolver.solve (_solve_bwd, amjax/multilevel.py:428-444).  Solves
  * A^T lam = gx (method 0: standalone cycles as amg_solve; 1: PCG as amg_pcg) on the
