@@ -358,6 +358,9 @@ class MultilevelSolver:
                                        return_info=return_info, method="pcg", atol=atol)
         prec = self._precision(precision)
         odt = torch.float32 if prec == N.PREC_F32 else torch.float64
+        if A is None and x0 is None and prec != N.PREC_F32 and _host_block(b, self.levels[0].A.shape[0]):
+            res, info = self._pcg_host(b, out, tol, atol, maxiter, cycle, cycles_per_level, prec)
+            return (res, info) if return_info else res
         bd, back = self._rhs(b, odt)
         A0 = self._override(A)
         if x0 is not None:
@@ -368,6 +371,40 @@ class MultilevelSolver:
             x = x + x0d
         res = _deliver(x, back, out)
         return (res, info) if return_info else res
+
+    def _pcg_host(self, b, out, tol, atol, maxiter, cycle, cycles_per_level, prec):
+        """PCG of a host [N, k] block through ``amg_pcg_host``: the columns are solved in two
+        blocks and each block's copy to and from the device overlaps the other's solve.
+        Pinned CPU tensors are used in place; other host inputs are staged through pinned
+        memory.  Returns the caller's kind (numpy in, numpy out; CPU tensor in, CPU tensor out)
+        or fills ``out``."""
+        n = self.levels[0].A.shape[0]
+        if isinstance(b, torch.Tensor):
+            bh, kind = b.detach(), "torch"
+            if bh.dtype != torch.float64 or not bh.is_contiguous():
+                bh = bh.to(torch.float64).contiguous()
+        else:
+            bh, kind = torch.from_numpy(np.ascontiguousarray(np.asarray(b, dtype=np.float64))), "numpy"
+        if not bh.is_pinned():
+            bh = bh.pin_memory()
+        k = int(bh.shape[1])
+        direct = (isinstance(out, torch.Tensor) and not out.is_cuda and out.dtype == torch.float64
+                  and out.is_contiguous() and out.numel() == n * k and out.is_pinned())
+        xh = out if direct else torch.empty((n, k), dtype=torch.float64).pin_memory()
+        if maxiter is None:
+            maxiter = 10 * n
+        iters = (C.c_int32 * k)()
+        rel = (C.c_double * k)()
+        blocks = 2 if k >= 16 else 1
+        N.call("amg_pcg_host", self._native(), prec, N.ptr(bh), N.ptr(xh), k, blocks, float(tol), float(atol),
+               int(maxiter), N.CYCLES[cycle], int(cycles_per_level), iters, rel, N.stream_ptr())
+        info = {"iterations": list(iters), "relres": list(rel)}
+        self.last_info = info
+        if out is not None:
+            if not direct:
+                out.copy_(xh.reshape(out.shape))
+            return out, info
+        return (xh.numpy() if kind == "numpy" else xh), info
 
     def _pcg_dev(self, bd, A0, tol, atol, maxiter, cycle, cycles_per_level, prec):
         h = self._native()
@@ -443,6 +480,15 @@ class MultilevelSolver:
         mt._transposed = self
         self._transposed = mt
         return mt
+
+
+def _host_block(b, n) -> bool:
+    """b is a host [n, k >= 2] block (numpy or a CPU tensor): the overlapped host path."""
+    if isinstance(b, torch.Tensor):
+        return (not b.is_cuda) and b.dim() == 2 and b.shape[0] == n and b.shape[1] >= 2
+    if isinstance(b, np.ndarray):
+        return b.ndim == 2 and b.shape[0] == n and b.shape[1] >= 2
+    return False
 
 
 def _deliver(x, back, out):

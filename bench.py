@@ -379,7 +379,8 @@ def run_ours(args):
         dist.all_reduce(te_tot, op=dist.ReduceOp.MAX)
     out["e2e"] = {"value": float(te_tot.item()) / (args.steps * world), "unit": "ms/solve",
                   "h2d_bytes_per_step": int(Bpin.numel() * 8), "d2h_bytes_per_step": int(Xpin.numel() * 8),
-                  "api": "MultilevelSolver.pcg(pinned host B, out=pinned host X, precision='mixed')"}
+                  "api": "MultilevelSolver.pcg(pinned host B, out=pinned host X, precision='mixed') -> "
+                         "amg_pcg_host: two column blocks, each block's copies overlapped with the other's solve"}
 
     # ---- variants (rank 0 only does the bookkeeping; every rank runs the same work)
     if not args.no_variants:
