@@ -239,6 +239,18 @@ struct HostStage {
     if (d2h) cudaStreamDestroy(d2h);
   }
 };
+// Zero-padded staging of requests whose column count is padded (pad_columns in amg_capi.cu):
+// right-hand sides and solution [n, kp].
+struct PadStage {
+  int dev = -1;
+  size_t bytes = 0;
+  void* b = nullptr;
+  void* x = nullptr;
+  ~PadStage() {
+    if (b) cudaFree(b);
+    if (x) cudaFree(x);
+  }
+};
 }  // namespace amg
 
 struct amg_hierarchy {
@@ -248,6 +260,7 @@ struct amg_hierarchy {
   std::map<std::string, std::unique_ptr<amg::Plan>> plans;
   std::mutex stage_mu;                     // one amg_pcg_host call at a time per hierarchy
   std::unique_ptr<amg::HostStage> stage;
+  std::unique_ptr<amg::PadStage> pad;      // guarded by mu
 };
 
 namespace amg {

@@ -395,7 +395,7 @@ class MultilevelSolver:
             maxiter = 10 * n
         iters = (C.c_int32 * k)()
         rel = (C.c_double * k)()
-        blocks = 2 if k >= 16 else 1
+        blocks = _host_blocks(k)
         N.call("amg_pcg_host", self._native(), prec, N.ptr(bh), N.ptr(xh), k, blocks, float(tol), float(atol),
                int(maxiter), N.CYCLES[cycle], int(cycles_per_level), iters, rel, N.stream_ptr())
         info = {"iterations": list(iters), "relres": list(rel)}
@@ -480,6 +480,15 @@ class MultilevelSolver:
         mt._transposed = self
         self._transposed = mt
         return mt
+
+
+def _host_blocks(k) -> int:
+    """Column blocks of a host-buffer PCG: 2 for k >= 16 (AMG_HOST_BLOCKS overrides)."""
+    import os
+    v = os.environ.get("AMG_HOST_BLOCKS")
+    if v and v.isdigit() and int(v) >= 1:
+        return min(int(v), k)
+    return 2 if k >= 16 else 1
 
 
 def _host_block(b, n) -> bool:

@@ -47,3 +47,23 @@ def test_host_block_pcg_pinned_out_and_torch_input():
     Xd = ml.pcg(B.cuda(), tol=1e-8, maxiter=200, precision="mixed")
     rel = float(torch.linalg.norm(out - Xd.cpu()) / torch.linalg.norm(Xd.cpu()))
     assert rel < 1e-6  # one k = 32 solve vs two k = 16 blocks: same columns, rounding of the sums
+
+
+@pytest.mark.parametrize("method", ["pcg", "solve"])
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_odd_k_runs_padded_to_the_vector_width(method, precision):
+    """k above 8 and not a multiple of 8 runs on ceil(k / 8) * 8 columns, the extra ones
+    zero (they retire at once): the k returned columns equal those of an explicit
+    zero-padded solve bit for bit, with the same iterations."""
+    A = gallery.poisson((40, 40))
+    ml = MultilevelSolver.from_pyamg(amg_setup.smoothed_aggregation_solver(A), presmoother=W23, postsmoother=W23)
+    B = np.random.default_rng(4).standard_normal((A.shape[0], 21))
+    Bp = np.zeros((A.shape[0], 24))
+    Bp[:, :21] = B
+    f = getattr(ml, method)
+    x, inf = f(torch.as_tensor(B).cuda(), tol=1e-9, maxiter=200, precision=precision, return_info=True)
+    xp, infp = f(torch.as_tensor(Bp).cuda(), tol=1e-9, maxiter=200, precision=precision, return_info=True)
+    assert x.shape == (A.shape[0], 21)
+    assert torch.equal(x, xp[:, :21])
+    assert list(inf["iterations"]) == list(infp["iterations"])[:21]
+    assert list(infp["iterations"])[21:] == [0, 0, 0]
