@@ -1170,18 +1170,13 @@ struct OpCgUpdA {
     }
   }
   // reliable: the CG of the reliable-update form (x and r are the FP32 increment and
-  // residual; retiring columns is left to the FP64 true residual).  has_cond: also set the
-  // graph's IF condition `cond` to "a true residual is due" (the refresh kernels then
-  // launch only when they have work).
+  // residual; retiring columns is left to the FP64 true residual)
   bool reliable = false;
-  int has_cond = 0;
-  cudaGraphConditionalHandle cond = 0;
   __device__ __forceinline__ int finalize_col(int c, double s) const {
     return reliable ? ctl.cg_col_ru(c, s) : ctl.cg_col(c, s);
   }
   __device__ __forceinline__ void finalize_all(int any) const {
     if (!reliable) ctl.set_any(any);
-    else if (has_cond) cudaGraphSetConditional(cond, ctl.ru[0] ? 1u : 0u);
   }
 };
 

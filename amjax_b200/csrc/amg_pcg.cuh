@@ -148,19 +148,12 @@ void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Em
     NvtxRange nv("amg/cg-step");
     OpCgQDir<TC, TC> qop{p_old, z, p_new, pl->beta(), k, pl->stop(), pl->gamma(), pl->alpha()};
     run_csr(*A0, qop, k, red_of(pl), cs, {p_old, z, p_new});
-    // in a graph, the refresh is an IF node whose condition the CG update sets; launched
-    // directly (no capture) the refresh kernels return at once unless due
-    cudaGraphConditionalHandle hc = 0;
-    const bool in_graph = cond_handle(cs, &hc);
     OpCgUpdA<TC, TC> up{};
     up.x = xs; up.r = rs; up.p = p_new; up.r_lo = nullptr;
     up.alpha = pl->alpha(); up.active = pl->active(); up.ld = k; up.stop = pl->stop();
     up.ctl = ctl; up.reliable = true;
-    up.has_cond = in_graph ? 1 : 0;
-    up.cond = hc;
     run_csr(*A0, up, k, red_of(pl), cs, {xs, rs, p_new});
-    if (in_graph) capture_if(cs, hc, true_residual);
-    else true_residual(cs);
+    true_residual(cs);
     cycle(cs);
   };
   *pro = [=](cudaStream_t cs) {

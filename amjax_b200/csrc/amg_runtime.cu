@@ -322,59 +322,6 @@ static cudaStream_t capture_stream() {
   return s;
 }
 
-// A second private stream for capturing a conditional node's body while the first is
-// still capturing its parent.
-static cudaStream_t capture_stream2() {
-  static thread_local std::map<int, cudaStream_t> streams;
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  auto it = streams.find(dev);
-  if (it != streams.end()) return it->second;
-  cudaStream_t s;
-  CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  streams[dev] = s;
-  return s;
-}
-
-bool cond_handle(cudaStream_t cs, cudaGraphConditionalHandle* out) {
-  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-  cudaGraph_t g = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t nd = 0;
-  CK(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd));
-  if (st != cudaStreamCaptureStatusActive || !g) return false;
-  CK(cudaGraphConditionalHandleCreate(out, g, 0, cudaGraphCondAssignDefault));
-  return true;
-}
-
-void capture_if(cudaStream_t cs, cudaGraphConditionalHandle h, const Emit& body) {
-  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-  cudaGraph_t g = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t nd = 0;
-  CK(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd));
-  if (st != cudaStreamCaptureStatusActive || !g) fail(AMG_ERR_INVALID_ARG, "internal: capture_if outside a capture");
-  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-  cp.conditional.handle = h;
-  cp.conditional.type = cudaGraphCondTypeIf;
-  cp.conditional.size = 1;
-  cudaGraphNode_t node;
-  CK(cudaGraphAddNode(&node, g, deps, nd, &cp));
-  cudaGraph_t bg = cp.conditional.phGraph_out[0];
-  cudaStream_t s2 = capture_stream2();
-  CK(cudaStreamBeginCaptureToGraph(s2, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  try {
-    body(s2);
-  } catch (...) {
-    cudaGraph_t junk = bg;
-    cudaStreamEndCapture(s2, &junk);
-    throw;
-  }
-  cudaGraph_t outg = bg;
-  CK(cudaStreamEndCapture(s2, &outg));
-  CK(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
-}
-
 template <class F>
 static cudaGraph_t capture(cudaGraph_t into, const cudaGraphNode_t* deps, size_t ndeps, F&& f) {
   cudaStream_t cs = capture_stream();

@@ -1141,12 +1141,6 @@ using Emit = std::function<void(cudaStream_t)>;
 Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s);
 void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& prologue,
               const Emit& body, const Emit& epilogue, bool has_loop, int gmax);
-// Conditional work inside a stream capture.  cond_handle: a handle on the graph that cs is
-// capturing into (false, no handle, when cs is not capturing).  capture_if: an IF node at
-// the capture's current position whose body is `body`, captured on a second stream; the
-// capture continues after the node.
-bool cond_handle(cudaStream_t cs, cudaGraphConditionalHandle* out);
-void capture_if(cudaStream_t cs, cudaGraphConditionalHandle h, const Emit& body);
 void read_results(Plan* pl, cudaStream_t s, bool cg, int32_t* iters_out, double* relres_out);
 LoopCtl make_ctl(Plan* pl, int maxiter);
 Red red_of(Plan* pl);
