@@ -65,13 +65,17 @@ static void pcg_batch_impl(amg_hierarchy* const* hs, int nsys, int precision, co
     BatchSys bs;
     bs.pl = pl;
     bs.gmax = maxiter + 2;
-    if constexpr (RU) pcg_ru_emit<TC>(hs[i], pl, q, s, &bs.pro, &bs.body, &bs.epi);
-    else pcg_emit<TO, TC>(hs[i], pl, q, s, &bs.pro, &bs.body);
+    const bool ru = RU && pr.k > 1;  // MIXED at k = 1 runs the FP64-CG form (faster there)
+    if (ru) {
+      if constexpr (RU) pcg_ru_emit<TC>(hs[i], pl, q, s, &bs.pro, &bs.body, &bs.epi);
+    } else {
+      pcg_emit<TO, TC>(hs[i], pl, q, s, &bs.pro, &bs.body);
+    }
     sys.push_back(std::move(bs));
     plans.push_back(pl);
     char buf[48];
     snprintf(buf, sizeof(buf), "/%p:", (void*)hs[i]);
-    key += buf + req_key(RU ? "pcg-ru" : "pcg", q);
+    key += buf + req_key(ru ? "pcg-ru" : "pcg", q);
   }
   run_batch(sys, key, s);
   size_t off = 0;
@@ -181,8 +185,8 @@ static void pcg_body(amg_hierarchy* h, int precision, const void* b, void* x, in
   q.program = true;
   if (precision == AMG_PREC_F64) pcg<double, double>(h, pl, q, s);
   else if (precision == AMG_PREC_F32) pcg<float, float>(h, pl, q, s);
-  else if (precision == AMG_PREC_MIXED && (!pa0 || pa0->v32)) pcg_ru(h, pl, q, s);
-  else pcg<double, float>(h, pl, q, s);
+  else if (precision == AMG_PREC_MIXED && pr.k > 1 && (!pa0 || pa0->v32)) pcg_ru(h, pl, q, s);
+  else pcg<double, float>(h, pl, q, s);  // MIXED_F64CG; MIXED at k = 1 (faster there)
   unpad_columns(h, pr, x, k, es, s);
   std::vector<int32_t> it(size_t(pr.k));
   std::vector<double> rr(size_t(pr.k));

@@ -8,7 +8,8 @@ benchmarks/benchmark.ipynb cell 7) is decided on the FP64 residual.  Checked aga
 plain FP64 PCG and the FP64-CG-around-FP32-cycle form ('mixed-f64cg') on the same
 hierarchy: FP64-checked residuals reach the tolerance, iteration counts stay within two
 of FP64's, solutions agree to the tolerance's accuracy, maxiter exhaustion reports the
-true residual, and zero / NaN columns retire at once without touching the others.
+true residual, and zero / NaN columns retire at once without touching the others.  (With
+one right-hand side 'mixed' runs the FP64-CG form, the faster one there.)
 """
 
 import numpy as np
@@ -51,8 +52,10 @@ def test_reliable_pcg_reaches_fp64_tolerance(kind, k, tol):
         assert abs(iru["iterations"][c] - i64["iterations"][c]) <= 2, (iru["iterations"], i64["iterations"])
         assert iru["relres"][c] <= tol
     # the reported relres of the reliable form is the FP64 true residual of the returned x
-    # (at 1e-10 the two summation orders of b - A x differ by ~1e-6 relative)
-    np.testing.assert_allclose(iru["relres"], _relres(A, b, xru), rtol=1e-4)
+    # (at 1e-10 the two summation orders of b - A x differ by ~1e-6 relative); with k = 1
+    # 'mixed' runs the FP64-CG form, which reports its recursive residual
+    if k > 1:
+        np.testing.assert_allclose(iru["relres"], _relres(A, b, xru), rtol=1e-4)
     assert rel(xru, x64) < 1e3 * tol
 
 
