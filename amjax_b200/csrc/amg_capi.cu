@@ -152,7 +152,8 @@ static void solve_body(amg_hierarchy* h, int precision, const void* b, void* x, 
   q.program = true;
   if (precision == AMG_PREC_F64) solve_plain<double>(h, pl, q, s);
   else if (precision == AMG_PREC_F32) solve_plain<float>(h, pl, q, s);
-  else solve_mixed(h, pl, q, s);
+  else if (precision == AMG_PREC_MIXED && (!pa0 || pa0->v32)) solve_mixed_ru(h, pl, q, s);
+  else solve_mixed(h, pl, q, s);  // MIXED_F64CG: FP64 refinement around the FP32 cycle
   unpad_columns(h, pr, x, k, es, s);
   std::vector<int32_t> it(size_t(pr.k));
   std::vector<double> rr(size_t(pr.k));

@@ -776,6 +776,28 @@ struct LoopCtl {
     ru[1] = 0;
     set_any(any);
   }
+
+  // ---- standalone solve with reliable updates (FP32 residual and increment; the rule of
+  // amjax/multilevel.py:414-422 decided on the FP64 norm).  thresh = tol * ||b||, nr the
+  // last norm; rmax keeps <r, r> (squared) for the delta test.
+  __device__ __forceinline__ int sa_col_ru(int c, double rr) const {
+    if (!active[c]) return 0;
+    iters[c] += 1;
+    const double n = sqrt(rr);
+    nr[c] = n;
+    ru[1] = 1;
+    if (n < thresh[c] || iters[c] >= maxiter || rr < delta2 * rmax[c] || !(rr == rr)) ru[0] = 1;
+    return 1;
+  }
+  __device__ __forceinline__ int true_col_sa(int c, double rr) const {
+    if (!active[c]) return 0;
+    const double n = sqrt(rr);
+    nr[c] = n;
+    rmax[c] = rr;
+    const int a = (n >= thresh[c]) && (iters[c] < maxiter);
+    active[c] = a;
+    return a;
+  }
 };
 
 // ------------------------------------------------------------------ x sources
@@ -915,9 +937,9 @@ struct OpJacobi {
 
 // r = b - A x (x from an XSource).  RLO: also/instead store a copy in another type.
 // NORM: reduce ||r||^2 per column and apply the standalone loop rule (outer loop of the
-// mixed-precision refinement), or with `true_rule` the CG rule of the reliable-update CG
-// (the FP64 true residual).  STORE: write r in T.  `gate` (nullable): the launch returns
-// at once unless *gate is set (the true residual runs only when one is due).
+// mixed-precision refinement), or with `true_rule` the rule of a reliable-update loop on the
+// FP64 true residual (1: CG, 2: standalone).  STORE: write r in T.  `gate` (nullable): the
+// launch returns at once unless *gate is set (the true residual runs only when one is due).
 template <class T, class VT, int XS, bool STORE, class TLO, bool NORM>
 struct OpResid {
   static constexpr bool kPrepared = false;
@@ -933,7 +955,7 @@ struct OpResid {
   const int* stop;
   LoopCtl ctl;
   const int* gate = nullptr;
-  bool true_rule = false;
+  int true_rule = 0;
 
   __device__ __forceinline__ bool stopped() const { return (stop && *stop) || (gate && !*gate); }
   __device__ __forceinline__ T x1(int j) const { return xs.get1(j); }
@@ -967,7 +989,11 @@ struct OpResid {
     }
   }
   __device__ __forceinline__ int finalize_col(int c, double s) const {
-    if constexpr (NORM) return true_rule ? ctl.true_col(c, s) : ctl.standalone_col(c, s);
+    if constexpr (NORM) {
+      if (true_rule == 1) return ctl.true_col(c, s);
+      if (true_rule == 2) return ctl.true_col_sa(c, s);
+      return ctl.standalone_col(c, s);
+    }
     return 1;
   }
   __device__ __forceinline__ void finalize_all(int any) const {
@@ -1180,6 +1206,72 @@ struct OpCgUpdA {
   }
 };
 
+// Standalone reliable-update step after a cycle e = M r: s = A e; for active columns
+// xs += e and r -= s (r stays the residual of x + xs); reduce <r, r> and apply the
+// standalone reliable rule (LoopCtl::sa_col_ru).
+template <class T>
+struct OpResUpd {
+  static constexpr bool kPrepared = false;
+  using V = T;
+  using Acc = T;
+  static constexpr bool kReduce = true;
+  __host__ __device__ __forceinline__ bool reduces() const { return kReduce; }
+  const T* e;
+  T* xs;
+  T* r;
+  const int* active;
+  int ld;
+  const int* stop;
+  LoopCtl ctl;
+
+  __device__ __forceinline__ bool stopped() const { return stop && *stop; }
+  __device__ __forceinline__ T x1(int j) const { return __ldg(e + j); }
+  template <int KV>
+  __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const {
+    ld_vec<T, KV>(e + voff(j, ld, c0), v);
+  }
+  __device__ __forceinline__ double epi1(int i, T s) const {
+    T rv = r[i];
+    if (active[0]) {
+      xs[i] = radd(xs[i], __ldg(e + i));
+      rv = rsub(rv, s);
+      r[i] = rv;
+    }
+    return rmul((double)rv, (double)rv);
+  }
+  template <int KV>
+  __device__ __forceinline__ void prek(int i, int c0, PreT<T, KV>& pp) const {
+    const size_t o = voff(i, ld, c0);
+    ld_vec<T, KV>(e + o, pp.x);
+    ld_vec<T, KV>(xs + o, pp.b);
+    ld_vec<T, KV>(r + o, pp.c);
+  }
+  template <int KV>
+  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>& pp,
+                                       double (&red)[KV]) const {
+    const size_t o = voff(i, ld, c0);
+    T xv[KV], rv[KV];
+    bool any = false;
+#pragma unroll
+    for (int v = 0; v < KV; ++v) {
+      xv[v] = pp.b[v];
+      rv[v] = pp.c[v];
+      if (active[c0 + v]) {
+        xv[v] = radd(xv[v], pp.x[v]);
+        rv[v] = rsub(rv[v], s[v]);
+        any = true;
+      }
+      red[v] = rfma((double)rv[v], (double)rv[v], red[v]);
+    }
+    if (any) {
+      st_vec<T, KV>(xs + o, xv);
+      st_vec<T, KV>(r + o, rv);
+    }
+  }
+  __device__ __forceinline__ int finalize_col(int c, double s) const { return ctl.sa_col_ru(c, s); }
+  __device__ __forceinline__ void finalize_all(int) const {}
+};
+
 // ------------------------------------------------------------------ elementwise ops
 // Reliable-update fold: x += xs (FP64 solution += FP32 increment), xs = 0, every column
 // (retired columns hold a zero increment).  Runs only when *gate is set.
@@ -1321,6 +1413,8 @@ struct OpJac0 {
 //   dst = src (T), dst_lo = src (TLO) ; sums[c] = sum src^2 ; loop set-up.
 // MODE 0: store the norm  sqrt(sum) (0 -> 1 guard) * tol into thresh, reset the loop.
 // MODE 1: CG set-up: thresh = max(tol^2 sum, atol^2), nr = sum, active = sum > thresh.
+// MODE 2: standalone reliable-update set-up: MODE 0's threshold, and the loop's first test
+//         ||b|| >= tol ||b|| (x0 = 0) applied here, with rmax = sum.
 template <class T, class TLO, int MODE>
 struct OpSetup {
   static constexpr bool kReduce = true;
@@ -1373,6 +1467,14 @@ struct OpSetup {
       nr[c] = sqrt(s);
       active[c] = 1;
       return 1;
+    } else if constexpr (MODE == 2) {
+      const double t = tol * nb;
+      thresh[c] = t;
+      nr[c] = sqrt(s);
+      if (rmax) rmax[c] = s;
+      const int a = (sqrt(s) >= t) && (maxiter > 0);
+      active[c] = a;
+      return a;
     } else {
       const double t = fmax(tol * tol * s, atol * atol);
       thresh[c] = t;

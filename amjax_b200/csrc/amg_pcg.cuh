@@ -141,7 +141,7 @@ void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Em
     OpResid<double, double, XS_PLAIN, false, TC, true> tr{};
     tr.xs = XSource<double, XS_PLAIN>{x, b, nullptr, 1.0, k};
     tr.b = b; tr.out = nullptr; tr.out_lo = rs; tr.ld = k; tr.stop = pl->stop();
-    tr.ctl = ctl; tr.gate = pl->ru(); tr.true_rule = true;
+    tr.ctl = ctl; tr.gate = pl->ru(); tr.true_rule = 1;
     run_csr(*A0, tr, k, red_of(pl), cs, {x, b, rs});
   };
   auto step = [=](cudaStream_t cs, TC* p_old, TC* p_new) {
@@ -210,7 +210,7 @@ void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Em
     OpResid<double, double, XS_PLAIN, false, TC, true> tr{};
     tr.xs = XSource<double, XS_PLAIN>{static_cast<const double*>(pl->q_out), b, nullptr, 1.0, k};
     tr.b = b; tr.out = nullptr; tr.out_lo = rs; tr.ld = k; tr.stop = nullptr;
-    tr.ctl = ctl; tr.true_rule = true;
+    tr.ctl = ctl; tr.true_rule = 1;
     tune_op(*A0, tr, k, red_of(pl), user, {pl->q_out, b, rs}, reset);
   }
 }

@@ -162,7 +162,7 @@ extern "C" amg_status amg_time_pcg_ops(amg_hierarchy* h, int32_t k, int32_t reps
           OpResid<double, double, XS_PLAIN, false, float, true> op{};
           op.xs = XSource<double, XS_PLAIN>{b.x64, b.b64, nullptr, 1.0, k};
           op.b = b.b64; op.out = nullptr; op.out_lo = b.rs; op.ld = k; op.stop = nullptr;
-          op.ctl = ctl; op.true_rule = true;
+          op.ctl = ctl; op.true_rule = 1;
           return op;
         };
         tune_op(A, mk(set[0]), k, red, s, {set[0].x64, set[0].b64, set[0].rs});

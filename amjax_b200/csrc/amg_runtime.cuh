@@ -1206,6 +1206,7 @@ inline void emit_setup(Plan* pl, cudaStream_t cs, int n0, const T* b, T* dst, TL
 // ------------------------------------------------------------------ drivers
 template <class T> void solve_plain(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 void solve_mixed(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
+void solve_mixed_ru(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 template <class TO, class TC> void pcg(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user);
 template <class TO, class TC>
 void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit* pro, Emit* bod);

@@ -50,16 +50,19 @@ typedef enum { AMG_CYCLE_V = 0, AMG_CYCLE_W = 1, AMG_CYCLE_F = 2 } amg_cycle;
  *  F32:   FP32 hierarchy end to end (the reference's dtype=float32 mode); sums that
  *         decide convergence are accumulated in FP64.
  *  MIXED: the cycle runs on FP32 values and vectors with FP32 accumulation.  Standalone
- *         solve: FP64 iterative refinement around the FP32 cycle (residual b - A x, update
- *         and convergence norm in FP64 on FP64 values).  PCG: CG with reliable updates:
+ *         solve: the residual and the solution increment are FP32, updated after every
+ *         cycle (r -= A e); the FP64 solution and the FP64 true residual b - A x are
+ *         brought up to date under the same rule as PCG's, and a column stops only on
+ *         the FP64 norm (the reference's rule).  PCG: CG with reliable updates:
  *         the CG vectors are FP32 (dot products and step lengths FP64); the FP64 solution
  *         and the FP64 true residual b - A x are brought up to date whenever the FP32
  *         residual has dropped by a fixed factor (AMG_RU_DELTA, default 1e-2) and before
  *         any column stops, so the stop rule is checked on the FP64 residual.  (With an
  *         A0 that has no FP32 values, and at k = 1, where its two extra launches per step
  *         outweigh the FP64 vector traffic it saves, PCG runs the MIXED_F64CG form.)
- *  MIXED_F64CG: as MIXED, except that PCG keeps its vectors in FP64 around the FP32
- *         cycle (FP64 CG preconditioned by the FP32 cycle). */
+ *  MIXED_F64CG: the FP32 cycle inside FP64 outer loops: standalone, FP64 iterative
+ *         refinement (residual b - A x, update and norm in FP64 every cycle); PCG, an FP64
+ *         CG preconditioned by the FP32 cycle. */
 typedef enum {
   AMG_PREC_F64 = 0,
   AMG_PREC_F32 = 1,

@@ -99,3 +99,28 @@ def test_reliable_pcg_batch_matches_single_solves():
         xs, i1 = m.pcg(b, tol=1e-9, maxiter=200, precision="mixed", return_info=True)
         assert torch.equal(x.reshape(xs.shape), xs)
         assert list(inf["iterations"]) == list(i1["iterations"])
+
+
+@pytest.mark.parametrize("kind", ["poisson", "lognormal"])
+@pytest.mark.parametrize("k", [1, 8])
+def test_reliable_standalone_solve(kind, k):
+    """The mixed standalone solve in its reliable-update form: FP32 residual and increment
+    updated after every cycle, FP64 refreshes, columns stopping on the FP64 norm with the
+    reference's rule (amjax/multilevel.py:414-422): iterations within one of the FP64
+    solve's, the tolerance reached on the FP64 residual, the reported relres the true one;
+    maxiter exhaustion stops every column at maxiter with its true residual."""
+    A, ml = _ml(64, kind)
+    B = np.random.default_rng(9).standard_normal((A.shape[0], k))
+    b = B[:, 0] if k == 1 else B
+    x64, i64 = ml.solve(b, tol=1e-9, maxiter=300, return_info=True)
+    x, inf = ml.solve(b, tol=1e-9, maxiter=300, precision="mixed", return_info=True)
+    r = _relres(A, b, x)
+    assert np.all(r < 1e-9), r.max()
+    for c in range(k):
+        assert abs(inf["iterations"][c] - i64["iterations"][c]) <= 1, (inf["iterations"], i64["iterations"])
+    np.testing.assert_allclose(inf["relres"], r, rtol=1e-4)
+    assert rel(x, x64) < 1e-6
+    xm, im = ml.solve(b, tol=1e-14, maxiter=4, precision="mixed", return_info=True)
+    assert im["iterations"] == [4] * k
+    np.testing.assert_allclose(im["relres"], _relres(A, b, xm), rtol=1e-4)
+    assert rel(xm, ml.solve(b, tol=1e-14, maxiter=4)) < 1e-5
