@@ -26,18 +26,20 @@ static PadReq pad_columns(amg_hierarchy* h, const void* b, void* x, int k, size_
   const size_t bytes = std::max<size_t>(size_t(n) * kp * es, 256);
   int dev = 0;
   CK(cudaGetDevice(&dev));
-  if (!h->pad || h->pad->dev != dev || h->pad->bytes < bytes) {
-    h->pad.reset();
+  std::unique_ptr<PadStage>& slot = h->pads[s];
+  if (!slot || slot->dev != dev || slot->bytes < bytes) {
+    if (slot) CK(cudaStreamSynchronize(s));  // the old staging may still be read on s
+    slot.reset();
     auto p = std::make_unique<PadStage>();
     p->dev = dev;
     p->bytes = bytes;
     CK(cudaMalloc(&p->b, bytes));
     CK(cudaMalloc(&p->x, bytes));
-    h->pad = std::move(p);
+    slot = std::move(p);
   }
-  CK(cudaMemcpy2DAsync(h->pad->b, kp * es, b, k * es, k * es, size_t(n), cudaMemcpyDeviceToDevice, s));
-  CK(cudaMemset2DAsync(static_cast<char*>(h->pad->b) + k * es, kp * es, 0, (kp - k) * es, size_t(n), s));
-  return PadReq{h->pad->b, h->pad->x, kp};
+  CK(cudaMemcpy2DAsync(slot->b, kp * es, b, k * es, k * es, size_t(n), cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemset2DAsync(static_cast<char*>(slot->b) + k * es, kp * es, 0, (kp - k) * es, size_t(n), s));
+  return PadReq{slot->b, slot->x, kp};
 }
 
 // Copy the first k solution columns back and the per-column results of those columns.

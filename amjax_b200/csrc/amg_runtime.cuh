@@ -260,7 +260,9 @@ struct amg_hierarchy {
   std::map<std::string, std::unique_ptr<amg::Plan>> plans;
   std::mutex stage_mu;                     // one amg_pcg_host call at a time per hierarchy
   std::unique_ptr<amg::HostStage> stage;
-  std::unique_ptr<amg::PadStage> pad;      // guarded by mu
+  // padded-request staging per stream (work on one stream is ordered, so a stream's
+  // staging is never in use by two requests at once); guarded by mu
+  std::map<cudaStream_t, std::unique_ptr<amg::PadStage>> pads;
 };
 
 namespace amg {

@@ -67,3 +67,22 @@ def test_odd_k_runs_padded_to_the_vector_width(method, precision):
     assert torch.equal(x, xp[:, :21])
     assert list(inf["iterations"]) == list(infp["iterations"])[:21]
     assert list(infp["iterations"])[21:] == [0, 0, 0]
+
+
+def test_host_block_pcg_refuses_f32_and_null():
+    import ctypes as C
+    from amjax_b200 import _native as N
+    A = gallery.poisson((20, 20))
+    ml = MultilevelSolver.from_pyamg(amg_setup.smoothed_aggregation_solver(A), presmoother=W23, postsmoother=W23)
+    B = torch.zeros(A.shape[0], 4, dtype=torch.float64).pin_memory()
+    X = torch.empty_like(B).pin_memory()
+    lib = N.load()
+    st = lib.amg_pcg_host(ml._native(), N.PREC_F32, N.ptr(B), N.ptr(X), 4, 2, 1e-8, 0.0, 10, 0, 1, None, None,
+                          N.stream_ptr())
+    assert st == 2
+    st = lib.amg_pcg_host(ml._native(), N.PREC_F64, None, N.ptr(X), 4, 2, 1e-8, 0.0, 10, 0, 1, None, None,
+                          N.stream_ptr())
+    assert st == 1
+    st = lib.amg_pcg_host(ml._native(), N.PREC_F64, N.ptr(B), N.ptr(X), 4, 0, 1e-8, 0.0, 10, 0, 1, None, None,
+                          N.stream_ptr())
+    assert st == 1
