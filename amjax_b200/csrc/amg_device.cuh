@@ -801,11 +801,18 @@ struct LoopCtl {
 };
 
 // ------------------------------------------------------------------ x sources
-enum XSrc { XS_PLAIN = 0, XS_JAC0 = 1, XS_ZERO = 2 };
+enum XSrc { XS_PLAIN = 0, XS_JAC0 = 1, XS_ZERO = 2, XS_RESJ0 = 3, XS_PROJ0 = 4 };
 
 // x_j as the SpMV sees it: the stored x, or one damped-Jacobi sweep from zero computed
 // on the fly, x_j = omega * (dinv_j * b_j) (relaxation.py:94-96 with x = 0: the SpMV of
 // the zero vector is exactly zero, so this is bit-identical to running the sweep).
+// Two-hop sources, used with one right-hand side (where a cycle is latency-bound and
+// recomputing a neighbour's value costs less than a launch), evaluated per gathered row
+// from an inner CSR matrix M (mrp / mci / mv):
+//   XS_RESJ0: x_j = b_j - sum_m M_jm x1_m, x1 = omega D^-1 b: the residual of the
+//             one-sweep-from-zero iterate (M = A): restriction R r without storing r;
+//   XS_PROJ0: x_j = x1_j + sum_J M_jJ xc_J (M = P): the prolonged and corrected iterate,
+//             so the post-smoothing sweep needs no stored x1 + P xc.
 template <class T, int XS>
 struct XSource {
   const T* x;
@@ -813,13 +820,31 @@ struct XSource {
   const T* dinv;
   T omega;
   int ld;
+  const int* mrp = nullptr;
+  const int* mci = nullptr;
+  const T* mv = nullptr;
+  const T* xc = nullptr;
+  __device__ __forceinline__ T jac0(int j) const { return rmul(omega, rmul(__ldg(dinv + j), __ldg(b + j))); }
   __device__ __forceinline__ T get1(int j) const {
     if constexpr (XS == XS_PLAIN) return __ldg(x + j);
-    else if constexpr (XS == XS_JAC0) return rmul(omega, rmul(__ldg(dinv + j), __ldg(b + j)));
-    else return T(0);
+    else if constexpr (XS == XS_JAC0) return jac0(j);
+    else if constexpr (XS == XS_RESJ0) {
+      T acc = T(0);
+      const int e = __ldg(mrp + j + 1);
+      for (int nz = __ldg(mrp + j); nz < e; ++nz) acc = rfma(__ldg(mv + nz), jac0(__ldg(mci + nz)), acc);
+      return rsub(__ldg(b + j), acc);
+    } else if constexpr (XS == XS_PROJ0) {
+      T acc = jac0(j);
+      const int e = __ldg(mrp + j + 1);
+      for (int nz = __ldg(mrp + j); nz < e; ++nz) acc = rfma(__ldg(mv + nz), __ldg(xc + __ldg(mci + nz)), acc);
+      return acc;
+    } else {
+      return T(0);
+    }
   }
   template <int KV>
   __device__ __forceinline__ void getk(int j, int c0, T (&v)[KV]) const {
+    static_assert(XS != XS_RESJ0 && XS != XS_PROJ0, "two-hop sources serve one right-hand side");
     if constexpr (XS == XS_PLAIN) {
       ld_vec<T, KV>(x + voff(j, ld, c0), v);
     } else if constexpr (XS == XS_JAC0) {
@@ -845,6 +870,7 @@ struct XSource {
 template <class T, int XS>
 struct OpJacobi {
   static constexpr bool kPrepared = false;
+  static constexpr bool kOnlyK1 = XS == XS_RESJ0 || XS == XS_PROJ0;
   using V = T;
   using Acc = T;
   XSource<T, XS> xs;
@@ -1046,6 +1072,44 @@ struct OpAxpy {
   __device__ __forceinline__ void finalize_all(int) const {}
 };
 
+
+// out = M x with x from a (two-hop) x source, one right-hand side: the restriction of the
+// residual of the one-sweep-from-zero iterate in one pass (XS_RESJ0).
+template <class T, int XS>
+struct OpRestrictX {
+  static constexpr bool kPrepared = false;
+  static constexpr bool kOnlyK1 = true;
+  using V = T;
+  using Acc = T;
+  static constexpr bool kReduce = false;
+  __host__ __device__ __forceinline__ bool reduces() const { return kReduce; }
+  XSource<T, XS> xs;
+  T* out;
+  int ld;
+  const int* stop;
+  __device__ __forceinline__ bool stopped() const { return stop && *stop; }
+  __device__ __forceinline__ T x1(int j) const { return xs.get1(j); }
+  template <int KV>
+  __device__ __forceinline__ void xk(int j, int c0, T (&v)[KV]) const { xs.template getk<KV>(j, c0, v); }
+  __device__ __forceinline__ double epi1(int i, T s) const {
+    out[i] = s;
+    return 0.0;
+  }
+  template <int KV>
+  __device__ __forceinline__ void prek(int, int, PreT<T, KV>&) const {}
+  template <int KV>
+  __device__ __forceinline__ void epik(int i, int c0, const T (&s)[KV], const PreT<T, KV>&, double (&)[KV]) const {
+    st_vec<T, KV>(out + voff(i, ld, c0), s);
+  }
+  __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
+  __device__ __forceinline__ void finalize_all(int) const {}
+};
+
+// Ops that serve one right-hand side only (two-hop sources) declare kOnlyK1.
+template <class Op, class = void>
+struct only_k1 : std::false_type {};
+template <class Op>
+struct only_k1<Op, std::void_t<decltype(Op::kOnlyK1)>> : std::bool_constant<Op::kOnlyK1> {};
 
 // CG step with the direction update folded in: p_new = z + beta p_old (z in the cycle's
 // type, beta per column from the last cycle) is formed on the fly for every gathered row

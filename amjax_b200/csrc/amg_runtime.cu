@@ -32,6 +32,23 @@ DevInfo dev_info() {
   return d;
 }
 
+bool fuse2_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("AMG_FUSE2");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+int fuse2_from() {
+  static const int v = [] {
+    const char* e = std::getenv("AMG_FUSE2_FROM");
+    const int x = e ? atoi(e) : 0;
+    return x >= 0 ? x : 0;
+  }();
+  return v;
+}
+
 bool nvtx_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("AMG_NVTX");

@@ -446,6 +446,10 @@ struct Red {
 // predecessor on the stream drains; every kernel of this library begins with
 // griddepcontrol.wait, so correctness does not depend on it.  AMG_PDL=0 disables.
 bool pdl_enabled();
+// Two-pass levels for one right-hand side (Cycle::visit): on unless AMG_FUSE2=0; from level
+// AMG_FUSE2_FROM (default 0) down.
+bool fuse2_enabled();
+int fuse2_from();
 
 template <class... Exp, class... Act>
 static void launch(void (*kernel)(Exp...), int grid, int block, size_t smem, cudaStream_t s,
@@ -574,6 +578,19 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
   const Cfg c = cfg_k<typename Op::Acc>(M.n_rows, k, M.g1, ptrs, M.rowptr, M.nnz, op_tag_for(op), op_tag<Op>());
   RedCtx rc{red.partials, red.counter, k};
   if (op.reduces() && !red.partials) fail(AMG_ERR_INVALID_ARG, "reduction scratch missing");
+  if constexpr (only_k1<Op>::value) {  // two-hop sources: one right-hand side, csr_k1 only
+    if (k != 1) fail(AMG_ERR_INVALID_ARG, "internal: a one-column op with k = %d", k);
+    switch (c.G) {
+      case 1: launch_k1<Op, 1>(M, vals, op, c, rc, s); break;
+      case 2: launch_k1<Op, 2>(M, vals, op, c, rc, s); break;
+      case 4: launch_k1<Op, 4>(M, vals, op, c, rc, s); break;
+      case 8: launch_k1<Op, 8>(M, vals, op, c, rc, s); break;
+      case 16: launch_k1<Op, 16>(M, vals, op, c, rc, s); break;
+      default: launch_k1<Op, 32>(M, vals, op, c, rc, s); break;
+    }
+    CK_LAUNCH();
+    return;
+  } else {
   if (k == 1) {
     switch (c.G) {
       case 1: launch_k1<Op, 1>(M, vals, op, c, rc, s); break;
@@ -617,6 +634,7 @@ static void run_csr(const Csr& M, const Op& op, int k, const Red& red, cudaStrea
     else fail(AMG_ERR_INVALID_ARG, "internal: 4-wide FP64 vectors");
   }
   CK_LAUNCH();
+  }
 }
 
 // ------------------------------------------------------------------ autotuner
@@ -757,6 +775,16 @@ void autotune_cycle(amg_hierarchy* h, Plan* pl, int k, const Csr* A0, cudaStream
       op.base = XSource<T, XS_JAC0>{nullptr, bl, dv, T(0.5), k};
       op.x = xc; op.out = w1; op.ld = k;
       tune_op(lv.P, op, k, Red{}, s, {bl, xc, w1});
+    }
+    if (k == 1 && fuse2_enabled()) {  // the two-pass level ops
+      OpRestrictX<T, XS_RESJ0> rop{};
+      rop.xs = XSource<T, XS_RESJ0>{nullptr, bl, dv, T(0.5), k, A.rowptr, A.col, A.template vals<T>(), nullptr};
+      rop.out = bc; rop.ld = k;
+      tune_op(lv.R, rop, k, Red{}, s, {bl, bc});
+      OpJacobi<T, XS_PROJ0> op{};
+      op.xs = XSource<T, XS_PROJ0>{nullptr, bl, dv, T(0.5), k, lv.P.rowptr, lv.P.col, lv.P.template vals<T>(), xc};
+      op.b = bl; op.dinv = dv; op.omega = T(0.5); op.out = w2; op.ld = k;
+      tune_op(A, op, k, Red{}, s, {bl, w2});
     }
   }
 }
@@ -1075,6 +1103,43 @@ struct Cycle {
     T* w1 = W1(l);
     T* w2 = W2(l);
     const bool top = (l == 0);
+
+    // ---- one right-hand side, iterate zero, one pre- and one post-sweep: two passes per
+    // level instead of four (two-hop sources): b_c = R (B - A x1) with x1 = omega D^-1 B
+    // evaluated per gathered row, then, after the coarse correction, X = sweep(x1 + P x_c)
+    // with x1 + P x_c evaluated per gathered row.
+    if (k == 1 && x_zero && !rec && fuse2_enabled() && l >= fuse2_from() && lv.pre.on() && lv.pre.iters == 1 &&
+        lv.post.on() && lv.post.iters == 1 && lv.template dinv<T>()) {
+      const T* dv = lv.template dinv<T>();
+      const T om_pre = T(lv.pre.omega);
+      const Csr& A = Aof(l);
+      T* Bc = static_cast<T*>(pl->B[l + 1]);
+      T* Xc = static_cast<T*>(pl->X[l + 1]);
+      {
+        OpRestrictX<T, XS_RESJ0> rop{};
+        rop.xs = XSource<T, XS_RESJ0>{nullptr, B, dv, om_pre, k, A.rowptr, A.col, A.template vals<T>(), nullptr};
+        rop.out = Bc; rop.ld = k; rop.stop = stop;
+        run_csr(lv.R, rop, k, red, s, {B, Bc});
+      }
+      if (l == L() - 2) coarse_solve(Bc, Xc);
+      else if (ct == 'V') visit(l + 1, true, 'V', cpl);
+      else if (ct == 'W') { visit(l + 1, true, 'W', cpl); visit(l + 1, false, 'W', cpl); }
+      else { visit(l + 1, true, 'F', cpl); for (int i = 0; i < cpl; ++i) visit(l + 1, false, 'V', cpl); }
+      const bool mask = top && fine_mask, dot = top && fine_dot != nullptr;
+      OpJacobi<T, XS_PROJ0> op{};
+      op.xs = XSource<T, XS_PROJ0>{nullptr, B, dv, om_pre, k, lv.P.rowptr, lv.P.col, lv.P.template vals<T>(), Xc};
+      op.b = B; op.dinv = dv; op.omega = T(lv.post.omega); op.out = X; op.ld = k;
+      op.norm = 0;
+      op.active = mask ? pl->active() : nullptr;
+      op.stop = stop;
+      op.rdot64 = (dot && dot_is_f64) ? static_cast<const double*>(fine_dot) : nullptr;
+      op.rdot32 = (dot && !dot_is_f64) ? static_cast<const float*>(fine_dot) : nullptr;
+      op.ctl = ctl;
+      op.gamma = pl->gamma();
+      op.beta = pl->beta();
+      run_csr(A, op, k, red, s, {B, X, dot ? fine_dot : nullptr});
+      return;
+    }
 
     // ---- pre-smoothing (x1)
     XD<T> x1 = x_zero ? XD<T>::zero() : XD<T>::plain(X);
