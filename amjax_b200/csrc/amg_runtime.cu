@@ -40,11 +40,11 @@ bool fuse2_enabled() {
   return on;
 }
 
-int fuse2_from() {
+int fuse2_rows() {
   static const int v = [] {
-    const char* e = std::getenv("AMG_FUSE2_FROM");
-    const int x = e ? atoi(e) : 0;
-    return x >= 0 ? x : 0;
+    const char* e = std::getenv("AMG_FUSE2_ROWS");
+    const int x = e ? atoi(e) : 20000;
+    return x >= 0 ? x : 20000;
   }();
   return v;
 }

@@ -446,10 +446,13 @@ struct Red {
 // predecessor on the stream drains; every kernel of this library begins with
 // griddepcontrol.wait, so correctness does not depend on it.  AMG_PDL=0 disables.
 bool pdl_enabled();
-// Two-pass levels for one right-hand side (Cycle::visit): on unless AMG_FUSE2=0; from level
-// AMG_FUSE2_FROM (default 0) down.
+// Two-pass levels for one right-hand side (Cycle::visit): on unless AMG_FUSE2=0, for levels
+// of at most AMG_FUSE2_ROWS rows (default 20,000).  Measured at k = 1 on the Poisson 500²
+// SA hierarchy (levels of 250,000 / 41,750 / ~7,000 / ... rows), PCG mixed: unfused 1.288 ms,
+// fused from level 2 (~7,000 rows) 1.222 ms, from level 1 1.307 ms, from level 0 1.438 ms:
+// on large levels recomputing each neighbour's value costs more than the launch it saves.
 bool fuse2_enabled();
-int fuse2_from();
+int fuse2_rows();
 
 template <class... Exp, class... Act>
 static void launch(void (*kernel)(Exp...), int grid, int block, size_t smem, cudaStream_t s,
@@ -776,7 +779,7 @@ void autotune_cycle(amg_hierarchy* h, Plan* pl, int k, const Csr* A0, cudaStream
       op.x = xc; op.out = w1; op.ld = k;
       tune_op(lv.P, op, k, Red{}, s, {bl, xc, w1});
     }
-    if (k == 1 && fuse2_enabled()) {  // the two-pass level ops
+    if (k == 1 && fuse2_enabled() && lv.A.n_rows <= fuse2_rows()) {  // the two-pass level ops
       OpRestrictX<T, XS_RESJ0> rop{};
       rop.xs = XSource<T, XS_RESJ0>{nullptr, bl, dv, T(0.5), k, A.rowptr, A.col, A.template vals<T>(), nullptr};
       rop.out = bc; rop.ld = k;
@@ -1108,7 +1111,7 @@ struct Cycle {
     // level instead of four (two-hop sources): b_c = R (B - A x1) with x1 = omega D^-1 B
     // evaluated per gathered row, then, after the coarse correction, X = sweep(x1 + P x_c)
     // with x1 + P x_c evaluated per gathered row.
-    if (k == 1 && x_zero && !rec && fuse2_enabled() && l >= fuse2_from() && lv.pre.on() && lv.pre.iters == 1 &&
+    if (k == 1 && x_zero && !rec && fuse2_enabled() && lv.A.n_rows <= fuse2_rows() && lv.pre.on() && lv.pre.iters == 1 &&
         lv.post.on() && lv.post.iters == 1 && lv.template dinv<T>()) {
       const T* dv = lv.template dinv<T>();
       const T om_pre = T(lv.pre.omega);
