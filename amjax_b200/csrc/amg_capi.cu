@@ -521,7 +521,7 @@ int64_t amg_kernel_launch_count(void) {
   if (cudaDeviceSynchronize() != cudaSuccess) return -1;
   unsigned long long mine = 0;
   if (cudaMemcpyFromSymbol(&mine, g_kernel_count, sizeof(mine)) != cudaSuccess) return -1;
-  return int64_t(mine + count_f64() + count_f32() + count_mixed() + count_runtime() + count_program());
+  return int64_t(mine + count_f64() + count_f32() + count_mixed() + count_mixed_cg() + count_runtime() + count_program());
 }
 
 const char* amg_last_error(void) { return t_err.c_str(); }

@@ -1,4 +1,5 @@
-// amg_drv_mixed.cu -- mixed-precision drivers: FP32 cycle inside FP64 refinement / FP64 CG.
+// amg_drv_mixed.cu -- mixed-precision standalone drivers: FP32 cycle inside FP64 refinement,
+// and the reliable-update standalone solve.
 #include "amg_drivers.cuh"
 
 namespace amg {
@@ -114,18 +115,6 @@ void solve_mixed_ru(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user)
   }
   run_loop(pl, req_key("solve-ru", q), user, prologue, body, epilogue, true, q.maxiter + 2);
 }
-
-// Mixed-precision PCG in the reliable-update form (FP32 CG, FP64 solution and true
-// residual on demand).
-void pcg_ru(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user) {
-  Emit pro, bod, epi;
-  pcg_ru_emit<float>(h, pl, q, user, &pro, &bod, &epi);
-  run_loop(pl, req_key("pcg-ru", q), user, pro, bod, epi, true, q.maxiter + 2);
-}
-
-template void pcg<double, float>(amg_hierarchy*, Plan*, const Req&, cudaStream_t);
-template void pcg_ru_emit<float>(amg_hierarchy*, Plan*, const Req&, cudaStream_t, Emit*, Emit*, Emit*);
-template void pcg_emit<double, float>(amg_hierarchy*, Plan*, const Req&, cudaStream_t, Emit*, Emit*);
 
 unsigned long long count_mixed() {
   unsigned long long v = 0;

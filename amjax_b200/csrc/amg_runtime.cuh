@@ -1303,6 +1303,7 @@ template <class T> void precondition(amg_hierarchy* h, Plan* pl, const Req& q, c
 unsigned long long count_f64();
 unsigned long long count_f32();
 unsigned long long count_mixed();
+unsigned long long count_mixed_cg();
 unsigned long long count_runtime();
 unsigned long long count_capi();
 unsigned long long count_program();

@@ -19,7 +19,7 @@ PKG = HERE.parent
 ROOT = PKG.parent
 OUT = PKG / "libamg_b200.so"
 OBJDIR = HERE / "_build"
-SOURCES = ["amg_runtime.cu", "amg_drv_f64.cu", "amg_drv_f32.cu", "amg_drv_mixed.cu", "amg_capi.cu",
+SOURCES = ["amg_runtime.cu", "amg_drv_f64.cu", "amg_drv_f32.cu", "amg_drv_mixed.cu", "amg_drv_mixed_cg.cu", "amg_capi.cu",
            "amg_noalloc.cu", "amg_program.cu", "amg_profile.cu"]
 HEADERS = ["amg_device.cuh", "amg_runtime.cuh", "amg_pcg.cuh", "amg_drivers.cuh", "amg_program.cuh",
            str(ROOT / "include" / "amg_b200.h")]
