@@ -14,7 +14,9 @@ Each configuration runs in a child process because the switches are read once pe
 process; the two runs of a comparison read one tuning file that a first run has completed,
 so both launch the same lane layouts (with k = 1 the lanes that split a row's nonzeros set
 its summation order, and a process that tunes as it goes can meet an op before its
-reducing variant is tuned).
+reducing variant is tuned).  All three runs keep the four-pass form of every level
+(AMG_FUSE2=0): the program records that form, while a two-pass level (launches only) sums
+each on-the-fly residual in its own order.
 """
 
 import json
@@ -67,9 +69,10 @@ def _run(env_extra, script):
 def test_program_path_is_bit_identical_to_launches(tmp_path):
     script = SCRIPT.format(root=ROOT)
     tune = str(tmp_path / "tune.txt")
-    _run({"AMG_PROGRAM": "0", "AMG_TUNE_FILE": tune}, script)  # records every layout decision
-    with_prog = _run({"AMG_PROGRAM": "1", "AMG_TUNE_FILE": tune}, script)
-    without = _run({"AMG_PROGRAM": "0", "AMG_TUNE_FILE": tune}, script)
+    base = {"AMG_TUNE_FILE": tune, "AMG_FUSE2": "0"}
+    _run(dict(base, AMG_PROGRAM="0"), script)  # records every layout decision
+    with_prog = _run(dict(base, AMG_PROGRAM="1"), script)
+    without = _run(dict(base, AMG_PROGRAM="0"), script)
     fewer = with_prog.pop("launches")
     more = without.pop("launches")
     assert set(with_prog) == set(without)
