@@ -583,8 +583,8 @@ LoopCtl make_ctl(Plan* pl, int maxiter) {
 double ru_delta2() {
   static const double d2 = [] {
     const char* e = std::getenv("AMG_RU_DELTA");
-    double d = e ? atof(e) : 1e-2;
-    if (!(d > 0.0 && d < 1.0)) d = 1e-2;
+    double d = e ? atof(e) : 3e-3;
+    if (!(d > 0.0 && d < 1.0)) d = 3e-3;
     return d * d;
   }();
   return d2;

@@ -56,7 +56,7 @@ typedef enum { AMG_CYCLE_V = 0, AMG_CYCLE_W = 1, AMG_CYCLE_F = 2 } amg_cycle;
  *         the FP64 norm (the reference's rule).  PCG: CG with reliable updates:
  *         the CG vectors are FP32 (dot products and step lengths FP64); the FP64 solution
  *         and the FP64 true residual b - A x are brought up to date whenever the FP32
- *         residual has dropped by a fixed factor (AMG_RU_DELTA, default 1e-2) and before
+ *         residual has dropped by a fixed factor (AMG_RU_DELTA, default 3e-3) and before
  *         any column stops, so the stop rule is checked on the FP64 residual.  (With an
  *         A0 that has no FP32 values, and at k = 1, where its two extra launches per step
  *         outweigh the FP64 vector traffic it saves, PCG runs the MIXED_F64CG form.)
