@@ -529,9 +529,18 @@ def run_ragged(args):
     for A, b, x in zip(mats, rhs, X):
         bn, xn = b.cpu().numpy(), x.cpu().numpy()
         rel.append(float((np.linalg.norm(bn - A @ xn, axis=0) / np.linalg.norm(bn, axis=0)).max()))
+    # the byte model of every system's solve (as for the headline: FP32 cycle, FP64-outer model
+    # of the CG vectors) at its iteration count, summed: the batch's HBM floor
+    from amjax_b200 import bytemodel
+    model = sum(bytemodel.solve_bytes(bytemodel.level_stats(m), int(b.shape[1]), max(d["iterations"]),
+                                      method="pcg", cycle_s=4, outer_s=8)
+                for m, b, d in zip(mls, rhs, info))
+    peak, _ = load_peaks()
     line = {"mode": "ragged", "metric": "ms per batch of 24 hierarchies (mixed PCG to 1e-8)",
             "value": tb, "unit": "ms/batch", "ms_min": tbmin, "sequential_ms": tsq,
             "speedup_vs_sequential": tsq / tb, "systems": 24,
+            "bytes_model": model, "gbs_model_batch": model / (tbmin * 1e-3) / 1e9,
+            "gbs_model_sequential": model / (tsqmin * 1e-3) / 1e9, "peak_gbs": peak,
             "rows": [A.shape[0] for A in mats], "rhs": [k for _, k in draws],
             "total_rows": int(sum(A.shape[0] for A in mats)), "total_rhs": int(sum(k for _, k in draws)),
             "iterations_max": [max(d["iterations"]) for d in info], "relres_fp64_max": max(rel),
