@@ -26,6 +26,14 @@ static PadReq pad_columns(amg_hierarchy* h, const void* b, void* x, int k, size_
   const size_t bytes = std::max<size_t>(size_t(n) * kp * es, 256);
   int dev = 0;
   CK(cudaGetDevice(&dev));
+  if (!h->pads.count(s) && int(h->pads.size()) >= max_plans()) {  // free the least recently used stage
+    auto used = [](const std::unique_ptr<PadStage>& st) { return st ? st->last_use : 0; };
+    auto lru = h->pads.begin();
+    for (auto p = h->pads.begin(); p != h->pads.end(); ++p)
+      if (used(p->second) < used(lru->second)) lru = p;
+    CK(cudaDeviceSynchronize());
+    h->pads.erase(lru);
+  }
   std::unique_ptr<PadStage>& slot = h->pads[s];
   if (!slot || slot->dev != dev || slot->bytes < bytes) {
     if (slot) CK(cudaStreamSynchronize(s));  // the old staging may still be read on s
@@ -37,6 +45,7 @@ static PadReq pad_columns(amg_hierarchy* h, const void* b, void* x, int k, size_
     CK(cudaMalloc(&p->x, bytes));
     slot = std::move(p);
   }
+  slot->last_use = ++h->use_clock;
   CK(cudaMemcpy2DAsync(slot->b, kp * es, b, k * es, k * es, size_t(n), cudaMemcpyDeviceToDevice, s));
   CK(cudaMemset2DAsync(static_cast<char*>(slot->b) + k * es, kp * es, 0, (kp - k) * es, size_t(n), s));
   return PadReq{slot->b, slot->x, kp};

@@ -276,11 +276,31 @@ static std::string plan_key(int prec, int k, cudaStream_t s) {
   return buf;
 }
 
+int max_plans() {
+  static const int v = [] {
+    const char* e = std::getenv("AMG_MAX_PLANS");
+    const int x = e ? atoi(e) : 16;
+    return x >= 2 ? x : (e ? 2 : 16);
+  }();
+  return v;
+}
+
 Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s) {
   const std::string key = plan_key(prec, k, s);
   auto it = h->plans.find(key);
-  if (it != h->plans.end()) return it->second.get();
+  if (it != h->plans.end()) {
+    it->second->last_use = ++h->use_clock;
+    return it->second.get();
+  }
+  if (int(h->plans.size()) >= max_plans()) {  // free the least recently requested plan
+    auto lru = h->plans.begin();
+    for (auto p = h->plans.begin(); p != h->plans.end(); ++p)
+      if (p->second->last_use < lru->second->last_use) lru = p;
+    CK(cudaDeviceSynchronize());
+    h->plans.erase(lru);
+  }
   auto pl = std::make_unique<Plan>();
+  pl->last_use = ++h->use_clock;
   pl->prec = prec;
   pl->k = k;
   pl->stream = s;

@@ -188,6 +188,7 @@ struct Plan {
   bool used_program = false;          // some captured solve of this plan runs a program
   std::vector<void*> allocs;
   std::list<std::pair<std::string, std::unique_ptr<GraphEntry>>> graphs;  // LRU
+  uint64_t last_use = 0;              // the hierarchy's plan clock at this plan's last request
   int64_t nodes_outside = 0, nodes_body = 0;
 
   double* thresh() { return dscal; }
@@ -244,6 +245,7 @@ struct HostStage {
 struct PadStage {
   int dev = -1;
   size_t bytes = 0;
+  uint64_t last_use = 0;
   void* b = nullptr;
   void* x = nullptr;
   ~PadStage() {
@@ -257,11 +259,12 @@ struct amg_hierarchy {
   std::vector<amg::Level> levels;
   amg::Coarse coarse;
   std::mutex mu;
-  std::map<std::string, std::unique_ptr<amg::Plan>> plans;
+  std::map<std::string, std::unique_ptr<amg::Plan>> plans;  // at most max_plans(), LRU
+  uint64_t use_clock = 0;                  // orders plan and padding-stage requests (LRU)
   std::mutex stage_mu;                     // one amg_pcg_host call at a time per hierarchy
   std::unique_ptr<amg::HostStage> stage;
   // padded-request staging per stream (work on one stream is ordered, so a stream's
-  // staging is never in use by two requests at once); guarded by mu
+  // staging is never in use by two requests at once); guarded by mu; at most max_plans(), LRU
   std::map<cudaStream_t, std::unique_ptr<amg::PadStage>> pads;
 };
 
@@ -1209,6 +1212,10 @@ struct Cycle {
 // ------------------------------------------------------------------ runtime (amg_runtime.cu)
 using Emit = std::function<void(cudaStream_t)>;
 Plan* get_plan(amg_hierarchy* h, int prec, int k, cudaStream_t s);
+// Plans (and padding stages) a hierarchy keeps: AMG_MAX_PLANS, default 16, at least 2.  A
+// request for a new (precision, k, stream) beyond it frees the least recently requested one
+// after a device synchronisation (its graphs may still be running on its stream).
+int max_plans();
 void run_loop(Plan* pl, const std::string& key, cudaStream_t user, const Emit& prologue,
               const Emit& body, const Emit& epilogue, bool has_loop, int gmax);
 void read_results(Plan* pl, cudaStream_t s, bool cg, int32_t* iters_out, double* relres_out);
