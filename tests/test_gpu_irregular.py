@@ -4,7 +4,8 @@ diagonal shift so the matrix is SPD), with irregular row lengths (1-22 nonzeros:
 points keep only their diagonal) and smoothed-aggregation hierarchies of four levels with
 irregular aggregates, down to a coarsest level of 1-4 rows.
 
-* FP64 standalone solve: iterates after 1, 2 and 5 V-cycles within 1e-10 of the oracle's;
+* FP64 standalone solve: iterates after 1, 2 and 5 V-, W- and F-cycles within 1e-10 of the
+  oracle's; the same (V, PCG) on a Ruge-Stuben hierarchy of the same operator;
 * FP64 PCG: iterates after 1 and 3 steps within 1e-10 of the oracle's CG, and the converged
   iteration count within one of it;
 * mixed precision (k = 5): PCG and standalone reach the FP64-checked tolerance 1e-8.
@@ -58,15 +59,33 @@ def test_irregular_rows(problem):
     assert len(ml.levels) >= 3
 
 
-def test_solve_per_iterate_fp64(problem):
+@pytest.mark.parametrize("cycle", ["V", "W", "F"])
+def test_solve_per_iterate_fp64(problem, cycle):
     A, host, ml, seed = problem
     oml = oracle_ml(host)
     b = np.random.default_rng(seed).standard_normal(A.shape[0])
     hist = []
-    O.solve_loop(oml, b, tol=0.0, maxiter=5, cycle_type="V", history=hist)
+    O.solve_loop(oml, b, tol=0.0, maxiter=5, cycle_type=cycle, history=hist)
     for m in (1, 2, 5):
-        x = ml.solve(b, tol=0.0, maxiter=m, cycle="V")
+        x = ml.solve(b, tol=0.0, maxiter=m, cycle=cycle)
         assert rel(x, hist[m - 1]) < 1e-10, (m, rel(x, hist[m - 1]))
+
+
+def test_ruge_stuben_per_iterate_fp64(problem):
+    A, _, _, seed = problem
+    host = amg_setup.ruge_stuben_solver(A)
+    ml = MultilevelSolver.from_pyamg(host, presmoother=W, postsmoother=W)
+    oml = oracle_ml(host)
+    b = np.random.default_rng(seed + 30).standard_normal(A.shape[0])
+    hist = []
+    O.solve_loop(oml, b, tol=0.0, maxiter=4, cycle_type="V", history=hist)
+    for m in (1, 4):
+        x = ml.solve(b, tol=0.0, maxiter=m)
+        assert rel(x, hist[m - 1]) < 1e-10, (m, rel(x, hist[m - 1]))
+    hist = []
+    O.cg(A, b, tol=0.0, maxiter=3, M=O.aspreconditioner(oml), history=hist)
+    xm = ml.pcg(b, tol=0.0, maxiter=3)
+    assert rel(xm, hist[2]) < 1e-10
 
 
 def test_pcg_per_iterate_fp64(problem):
