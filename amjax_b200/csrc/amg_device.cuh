@@ -938,7 +938,15 @@ struct OpJacobi {
       for (int v = 0; v < KV; ++v) red[v] = rfma(rv[v], (double)y[v], red[v]);
     } else if (rdot32) {
       float rv[KV];
-      ld_vec<float, KV>(rdot32 + o, rv);
+      bool loaded = false;  // the CG's <r, z> with r the sweep's right-hand side: already in p.b
+      if constexpr (std::is_same<T, float>::value) {
+        if (rdot32 == b) {
+#pragma unroll
+          for (int v = 0; v < KV; ++v) rv[v] = p.b[v];
+          loaded = true;
+        }
+      }
+      if (!loaded) ld_vec<float, KV>(rdot32 + o, rv);
 #pragma unroll
       for (int v = 0; v < KV; ++v) red[v] = rfma((double)rv[v], (double)y[v], red[v]);
     }
@@ -1597,27 +1605,6 @@ struct OpMaskCopy {
     }
     return 1;
   }
-  __device__ __forceinline__ void finalize_all(int) const {}
-};
-
-// dst (type TD) = src (type TS), converting.
-template <class TD, class TS>
-struct OpConvert {
-  static constexpr bool kReduce = false;
-  __host__ __device__ __forceinline__ bool reduces() const { return kReduce; }
-  const TS* src;
-  TD* dst;
-  int ld;
-  const int* stop;
-  __device__ __forceinline__ bool stopped() const { return stop && *stop; }
-  template <int KV>
-  __device__ __forceinline__ void elem(int i, int c0, double (&)[KV]) const {
-    const size_t o = voff(i, ld, c0);
-    TD v[KV];
-    ld_cvt<TD, TS, KV>(src + o, v);
-    st_vec<TD, KV>(dst + o, v);
-  }
-  __device__ __forceinline__ int finalize_col(int, double) const { return 1; }
   __device__ __forceinline__ void finalize_all(int) const {}
 };
 

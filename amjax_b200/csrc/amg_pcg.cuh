@@ -52,9 +52,9 @@ void pcg_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Emit*
   *pro = [=](cudaStream_t cs) {
     emit_setup<TO, TC, 1>(pl, cs, n0, b, r, mixed ? rc : nullptr, x, tol, atol, maxiter);
     cycle(cs);
-    // first direction p = z: p_old = z and beta = 0 give z + 0 * z = z exactly
-    OpConvert<TO, TC> cp{z, pa, k, pl->stop()};
-    run_elem<TC>(n0, cp, k, red_of(pl), cs, {z, pa});
+    // first direction p = z: p_old = 0 and beta = 0 give fma(0, 0, z) = z (a memset node, not
+    // a pass that reads z)
+    CK(cudaMemsetAsync(pa, 0, sizeof(TO) * size_t(n0) * size_t(k), cs));
     CK(cudaMemsetAsync(pl->beta(), 0, sizeof(double) * size_t(k), cs));
   };
   *bod = [=](cudaStream_t cs) {
@@ -165,8 +165,7 @@ void pcg_ru_emit(amg_hierarchy* h, Plan* pl, const Req& q, cudaStream_t user, Em
     run_elem<TC>(n0, op, k, red_of(pl), cs, {b, rs, x});
     CK(cudaMemsetAsync(xs, 0, sizeof(TC) * size_t(n0) * size_t(k), cs));
     cycle(cs);
-    OpConvert<TC, TC> cp{z, pa, k, pl->stop()};
-    run_elem<TC>(n0, cp, k, red_of(pl), cs, {z, pa});
+    CK(cudaMemsetAsync(pa, 0, sizeof(TC) * size_t(n0) * size_t(k), cs));  // p_old = 0, beta = 0: p = z
     CK(cudaMemsetAsync(pl->beta(), 0, sizeof(double) * size_t(k), cs));
   };
   *bod = [=](cudaStream_t cs) {
