@@ -40,6 +40,24 @@ bool fuse2_enabled() {
   return on;
 }
 
+double fuse2_chain() {
+  static const double v = [] {
+    const char* e = std::getenv("AMG_FUSE2_CHAIN");
+    const double x = e ? atof(e) : 400.0;
+    return x >= 0.0 ? x : 400.0;
+  }();
+  return v;
+}
+
+double fuse2_work() {
+  static const double v = [] {
+    const char* e = std::getenv("AMG_FUSE2_WORK");
+    const double x = e ? atof(e) : 5e5;
+    return x >= 0.0 ? x : 5e5;
+  }();
+  return v;
+}
+
 int fuse2_rows() {
   static const int v = [] {
     const char* e = std::getenv("AMG_FUSE2_ROWS");

@@ -450,12 +450,29 @@ struct Red {
 // griddepcontrol.wait, so correctness does not depend on it.  AMG_PDL=0 disables.
 bool pdl_enabled();
 // Two-pass levels for one right-hand side (Cycle::visit): on unless AMG_FUSE2=0, for levels
-// of at most AMG_FUSE2_ROWS rows (default 20,000).  Measured at k = 1 on the Poisson 500²
-// SA hierarchy (levels of 250,000 / 41,750 / ~7,000 / ... rows), PCG mixed: unfused 1.288 ms,
-// fused from level 2 (~7,000 rows) 1.222 ms, from level 1 1.307 ms, from level 0 1.438 ms:
-// on large levels recomputing each neighbour's value costs more than the launch it saves.
+// of at most AMG_FUSE2_ROWS rows (default 20,000) whose two-hop gathers,
+// nnz(R) nnz(A) / n + nnz(A) nnz(P) / n, number at most AMG_FUSE2_WORK (default 500,000).
+// Measured at k = 1, PCG mixed, on the Poisson 500² SA hierarchy (levels of 250,000 /
+// 41,750 / 4,704 / 532 rows, two-hop gathers 6.2e6 / 2.1e6 / 2.3e5 / 2.4e4): unfused
+// 1.288 ms, fused from level 2 1.222 ms, from level 1 1.307 ms, from level 0 1.438 ms; and
+// on the 3D 128³ diffusion SA hierarchy (a level of 6,349 rows with 59 nonzeros per row,
+// 3.8e6 two-hop gathers) a V-cycle solve took 36.2 ms unfused and 83.6 ms with that level
+// fused: recomputing each neighbour's value costs more than the launch it saves unless
+// the level's gathers are few.  A coarse row's restriction also walks its two-hop gathers
+// in one lane group, so the mean per coarse row, nnz(R) / n_c * nnz(A) / n, must stay at
+// most AMG_FUSE2_CHAIN (default 400; Poisson 500² levels 2-4: 212 / 185 / 19; the 128³
+// hierarchy's 82-row level, whose two coarse rows hold 76 nonzeros each: 2,830, and fused
+// it cost 40.5 vs 36.2 ms).
 bool fuse2_enabled();
 int fuse2_rows();
+double fuse2_work();
+double fuse2_chain();
+inline bool fuse2_level(const Level& lv, const Csr& A, int k) {
+  if (k != 1 || !fuse2_enabled() || A.n_rows == 0 || A.n_rows > fuse2_rows() || lv.R.n_rows == 0) return false;
+  const double n = A.n_rows, a = double(A.nnz) / n;
+  if (double(lv.R.nnz) / double(lv.R.n_rows) * a > fuse2_chain()) return false;
+  return double(lv.R.nnz) * a + double(A.nnz) * (double(lv.P.nnz) / n) <= fuse2_work();
+}
 
 template <class... Exp, class... Act>
 static void launch(void (*kernel)(Exp...), int grid, int block, size_t smem, cudaStream_t s,
@@ -782,7 +799,7 @@ void autotune_cycle(amg_hierarchy* h, Plan* pl, int k, const Csr* A0, cudaStream
       op.x = xc; op.out = w1; op.ld = k;
       tune_op(lv.P, op, k, Red{}, s, {bl, xc, w1});
     }
-    if (k == 1 && fuse2_enabled() && lv.A.n_rows <= fuse2_rows()) {  // the two-pass level ops
+    if (fuse2_level(lv, A, k)) {  // the two-pass level ops
       OpRestrictX<T, XS_RESJ0> rop{};
       rop.xs = XSource<T, XS_RESJ0>{nullptr, bl, dv, T(0.5), k, A.rowptr, A.col, A.template vals<T>(), nullptr};
       rop.out = bc; rop.ld = k;
@@ -1110,11 +1127,11 @@ struct Cycle {
     T* w2 = W2(l);
     const bool top = (l == 0);
 
-    // ---- one right-hand side, iterate zero, one pre- and one post-sweep: two passes per
-    // level instead of four (two-hop sources): b_c = R (B - A x1) with x1 = omega D^-1 B
-    // evaluated per gathered row, then, after the coarse correction, X = sweep(x1 + P x_c)
-    // with x1 + P x_c evaluated per gathered row.
-    if (k == 1 && x_zero && !rec && fuse2_enabled() && lv.A.n_rows <= fuse2_rows() && lv.pre.on() && lv.pre.iters == 1 &&
+    // ---- one right-hand side on a small level (fuse2_level), iterate zero, one pre- and one
+    // post-sweep: two passes per level instead of four (two-hop sources): b_c = R (B - A x1)
+    // with x1 = omega D^-1 B evaluated per gathered row, then, after the coarse correction,
+    // X = sweep(x1 + P x_c) with x1 + P x_c evaluated per gathered row.
+    if (x_zero && !rec && fuse2_level(lv, Aof(l), k) && lv.pre.on() && lv.pre.iters == 1 &&
         lv.post.on() && lv.post.iters == 1 && lv.template dinv<T>()) {
       const T* dv = lv.template dinv<T>();
       const T om_pre = T(lv.pre.omega);
