@@ -10,6 +10,11 @@ computed per gathered row, so such a level runs two CSR passes instead of four.
   below 1e-4 in FP32.
 * The two-pass form launches fewer kernels.
 * AMG_FUSE2_ROWS=0 (no level qualifies) launches as many kernels as AMG_FUSE2=0.
+* The gather bounds: on a 16³ variable-diffusion SA hierarchy (levels of 4,096 / 514 / 18
+  rows; the 514-row level's restriction walks ~2,700 two-hop gathers per coarse row) the
+  default gate fuses levels 0 and 2 but not 1, so it launches more kernels than with the
+  bounds lifted (AMG_FUSE2_CHAIN, AMG_FUSE2_WORK) and fewer than with AMG_FUSE2=0; the
+  three give the same iteration counts and solutions agreeing to rounding.
 
 Each configuration runs in a child process because the switches are read once per process.
 """
@@ -81,3 +86,40 @@ def test_two_pass_levels_match_four_pass(runs):
 def test_two_pass_levels_launch_fewer_kernels(runs):
     assert runs["on"]["launches"] < runs["off"]["launches"]
     assert runs["none"]["launches"] == runs["off"]["launches"]
+
+
+DENSE = r"""
+import sys, json, numpy as np
+sys.path.insert(0, {root!r})
+from amjax_b200 import MultilevelSolver, amg_setup, gallery
+from amjax_b200 import _native as N
+W = ("jacobi", {{"iterations": 1, "omega": 2.0 / 3.0}})
+A = gallery.variable_diffusion_3d(16, sigma=1.0, seed=2)
+ml = MultilevelSolver.from_pyamg(amg_setup.smoothed_aggregation_solver(A), presmoother=W, postsmoother=W)
+b = np.random.default_rng(4).standard_normal(A.shape[0])
+ml.pcg(b, tol=1e-9, maxiter=100)  # tuning and capture outside the count
+n0 = N.kernel_launch_count()
+x, info = ml.pcg(b, tol=1e-9, maxiter=100, return_info=True)
+print(json.dumps({{"x": np.asarray(x).tolist(), "it": int(info["iterations"][0]),
+                  "launches": N.kernel_launch_count() - n0, "levels": [l.A.shape[0] for l in ml.levels]}}))
+"""
+
+
+def _run_dense(env_extra):
+    env = dict(os.environ, **env_extra)
+    r = subprocess.run([sys.executable, "-c", DENSE.format(root=ROOT)], env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_gather_bounds_exclude_dense_levels():
+    gated = _run_dense({})
+    lifted = _run_dense({"AMG_FUSE2_CHAIN": "1e12", "AMG_FUSE2_WORK": "1e12"})
+    off = _run_dense({"AMG_FUSE2": "0"})
+    assert gated["levels"][:3] == [4096, 514, 18]
+    assert lifted["launches"] < gated["launches"] < off["launches"]
+    assert gated["it"] == lifted["it"] == off["it"]
+    xo = np.asarray(off["x"])
+    for run in (gated, lifted):
+        assert np.linalg.norm(np.asarray(run["x"]) - xo) / np.linalg.norm(xo) < 1e-9
