@@ -1,5 +1,6 @@
 // amg_runtime.cu -- non-template host runtime: errors, device facts, plans, graph
 // construction (conditional WHILE node) and execution.
+#include <cmath>
 #include <tuple>
 
 #include "amg_runtime.cuh"
@@ -185,6 +186,33 @@ int resident_ctas(const void* fn, size_t smem) {
   nb = std::max(1, std::min(nb, 2048 / kBlock));
   cache[key] = nb;
   return nb;
+}
+
+int carveout_pct(const void* fn, size_t smem) {
+  static const bool on = [] {
+    const char* e = std::getenv("AMG_CARVEOUT");
+    return !(e && e[0] == '0');
+  }();
+  if (!on) return -1;
+  static std::mutex m;
+  static std::map<std::pair<const void*, size_t>, int> cache;
+  {
+    std::lock_guard<std::mutex> lk(m);
+    auto it = cache.find(std::make_pair(fn, smem));
+    if (it != cache.end()) return it->second;
+  }
+  const int per = resident_ctas(fn, smem);  // with the largest shared-memory share
+  cudaFuncAttributes fa{};
+  CK(cudaFuncGetAttributes(&fa, fn));
+  int dev = 0, sm_bytes = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  const double need = double(per) * (double(smem) + double(fa.sharedSizeBytes) + 1024.0);
+  int pct = sm_bytes > 0 ? int(std::ceil(100.0 * need / double(sm_bytes))) + 2 : -1;
+  if (pct > 100) pct = 100;
+  std::lock_guard<std::mutex> lk(m);
+  cache[std::make_pair(fn, smem)] = pct;
+  return pct;
 }
 
 void check_csr(const amg_csr& c, const char* what, int lvl) {
